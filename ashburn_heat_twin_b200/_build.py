@@ -1,0 +1,80 @@
+"""Build libahx.so (the CUDA backend, sm_100a) in-tree with nvcc.
+
+Translation units and their arithmetic flags:
+  step_exact.cu  -fmad=false  fused step, every f32 expression individually rounded (bit-identical to the CPU
+                              restatement of the reference kernels)
+  step_fast.cu   -fmad=true   fused step with multiply-add contraction
+  aux.cu         -fmad=false  read-back, init, re-init, stats, layout conversion
+  api.cu                      the C ABI (include/ahx.h)
+All use -ftz=true (f32 subnormals flushed, as the CPU restatement does) with IEEE division and square root.
+"""
+from __future__ import annotations
+
+import concurrent.futures as cf
+import glob
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, 'csrc')
+INCLUDE = os.path.join(os.path.dirname(HERE), 'include')
+LIB = os.path.join(HERE, 'libahx.so')
+OBJDIR = os.path.join(HERE, '_build')
+
+ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
+COMMON = ['-O3', '-std=c++17', '--expt-relaxed-constexpr', '-lineinfo', '-ftz=true', '-prec-div=true',
+          '-prec-sqrt=true', '-Xcompiler', '-fPIC', '-I', INCLUDE]
+UNITS = {
+    'step_exact.cu': ['-fmad=false'],
+    'step_fast.cu': ['-fmad=true'],
+    'aux.cu': ['-fmad=false'],
+    'api.cu': ['-fmad=false'],
+}
+
+
+def nvcc():
+    p = shutil.which('nvcc') or '/usr/local/cuda/bin/nvcc'
+    if not os.path.exists(p):
+        raise RuntimeError('nvcc not found: the CUDA toolkit is required to build libahx.so')
+    return p
+
+
+def _deps_mtime():
+    files = glob.glob(os.path.join(CSRC, '*')) + glob.glob(os.path.join(INCLUDE, '*.h')) + [__file__]
+    return max(os.path.getmtime(f) for f in files)
+
+
+def build(force: bool = False, verbose: bool = False, ptxas_v: bool = False) -> str:
+    """Compile (if out of date) and return the path of libahx.so."""
+    if not force and os.path.exists(LIB) and os.path.getmtime(LIB) >= _deps_mtime() and not ptxas_v:
+        return LIB
+    os.makedirs(OBJDIR, exist_ok=True)
+    cc = nvcc()
+
+    def one(unit):
+        obj = os.path.join(OBJDIR, unit.replace('.cu', '.o'))
+        cmd = [cc] + ARCH + COMMON + UNITS[unit] + (['-Xptxas', '-v'] if ptxas_v else []) + \
+            ['-c', os.path.join(CSRC, unit), '-o', obj]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f'nvcc failed on {unit}:\n{r.stderr[-6000:]}')
+        return obj, r.stderr
+
+    with cf.ThreadPoolExecutor(max_workers=len(UNITS)) as ex:
+        results = list(ex.map(one, UNITS))
+    if verbose or ptxas_v:
+        for _, err in results:
+            sys.stderr.write(err)
+    tmp = LIB + '.tmp'
+    cmd = [cc] + ARCH + ['-shared', '-o', tmp] + [o for o, _ in results] + ['-lcudart']
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f'link failed:\n{r.stderr[-4000:]}')
+    os.replace(tmp, LIB)
+    return LIB
+
+
+if __name__ == '__main__':
+    print(build(force='--force' in sys.argv, verbose=True, ptxas_v='-v' in sys.argv))

@@ -1,0 +1,834 @@
+// C ABI of the B200 live solver (include/ahx.h): handle lifetime, host images, stepping, asynchronous read-back,
+// diagnostics and budgets over the kernels of step_exact.cu / step_fast.cu / aux.cu.
+//
+// Device model: one CUDA stream per handle runs everything that touches the state, in submission order (the
+// reference's single WebGPU queue, solver.js:401-427). Read-back runs its two small kernels on that stream and copies
+// on a second stream, so a read never stalls stepping (solver.js:439-471). Host images are staged through a ring of
+// pinned buffers so an upload between steps does not wait for the GPU (the reference's queue.writeBuffer).
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/ahx.h"
+#include "launch.h"
+
+using namespace ahx;
+
+namespace {
+
+thread_local std::string g_err;
+
+ahx_status fail(ahx_status st, const std::string& msg) {
+  g_err = msg;
+  return st;
+}
+
+constexpr int kUploadSlots = 4;
+// column levels (kt, ktop) are validated against this bound so every level index stays a small non-negative int
+constexpr uint32_t kMaxLevel = 65535;
+
+struct ReadSlot {
+  bool busy = false;
+  uint64_t ticket = 0;
+  int nzv = 0, want_vol = 0, want_wind = 0;
+  float* d_surf = nullptr;     // 3*NXY
+  uint32_t* d_vol = nullptr;   // ceil(nz*NXY/4)
+  unsigned* d_tmax = nullptr;
+  float* h_surf = nullptr;     // pinned
+  uint8_t* h_vol = nullptr;    // pinned
+  unsigned* h_tmax = nullptr;  // pinned
+  cudaEvent_t ev_kernels = nullptr, ev_done = nullptr;
+};
+
+struct UploadSlot {
+  void* h = nullptr;   // pinned
+  size_t bytes = 0;
+  cudaEvent_t ev = nullptr;
+  bool used = false;
+};
+
+struct Fence {
+  uint64_t ticket;
+  cudaEvent_t ev;
+};
+
+}  // namespace
+
+struct ahx_handle {
+  std::mutex mu;
+  int dev = 0;
+  bool destroyed = false;
+  bool lost = false;
+  std::string lost_msg;
+  cudaStream_t s_step = nullptr, s_copy = nullptr;
+  ahx_dims dims{};
+  int esize = 4, px = 0;
+  uint32_t ps = 0, qs = 0;
+  void* f[2] = {nullptr, nullptr};
+  void* g[2] = {nullptr, nullptr};
+  unsigned char* d_params = nullptr;
+  uint4* d_colv = nullptr;
+  uint32_t* d_ktop = nullptr;
+  uint32_t* d_oldk = nullptr;
+  float4* d_dbg = nullptr;
+  double* d_budget = nullptr;
+  bool budget_on = false;
+  StatsScratch* d_stats = nullptr;
+  int parity = 0;
+  int64_t steps = 0;
+  int block_y = 4, zslab = 0;
+  ReadSlot reads[AHX_MAX_READS];
+  uint64_t next_read = 0;
+  UploadSlot up[kUploadSlots];
+  int up_next = 0;
+  std::vector<Fence> fences;
+  uint64_t next_fence = 0;
+  char name[64] = {0};
+};
+
+namespace {
+
+// mark the handle lost on a CUDA error; returns AHX_EDEVICE with the message
+ahx_status cuda_fail(ahx_handle* h, cudaError_t e, const char* what) {
+  std::string m = std::string(what) + ": " + cudaGetErrorString(e);
+  if (h) {
+    h->lost = true;
+    h->lost_msg = m;
+  }
+  return fail(AHX_EDEVICE, "live solver: CUDA error (" + m + ")");
+}
+
+#define AHX_CUDA(h, call)                                   \
+  do {                                                      \
+    cudaError_t e__ = (call);                               \
+    if (e__ != cudaSuccess) return cuda_fail(h, e__, #call); \
+  } while (0)
+
+ahx_status check(ahx_handle* h) {
+  if (!h) return fail(AHX_EINVAL, "live solver: null handle");
+  if (h->destroyed) return fail(AHX_EDESTROYED, "live solver: destroyed");
+  if (h->lost) return fail(AHX_EDEVICE, "live solver: CUDA device lost (" + h->lost_msg + ")");
+  return AHX_OK;
+}
+
+size_t nxy(const ahx_handle* h) { return (size_t)h->dims.nx * h->dims.ny; }
+size_t ncells(const ahx_handle* h) { return nxy(h) * h->dims.nz; }
+size_t params_bytes(const ahx_handle* h) { return 64 + 16 * (size_t)h->dims.nz; }
+
+DomainView view(ahx_handle* h) {
+  DomainView D;
+  D.params = h->d_params;
+  D.colv = h->d_colv;
+  D.ktop = h->d_ktop;
+  D.fA = h->f[h->parity];
+  D.fB = h->f[1 - h->parity];
+  D.gA = h->g[h->parity];
+  D.gB = h->g[1 - h->parity];
+  D.dbg = h->d_dbg;
+  D.budget = h->d_budget;
+  D.nx = h->dims.nx;
+  D.ny = h->dims.ny;
+  D.nz = h->dims.nz;
+  D.px = h->px;
+  D.ps = h->ps;
+  D.qs = h->qs;
+  return D;
+}
+
+// copy a host image to device memory in stream order without blocking the host on the GPU
+ahx_status upload(ahx_handle* h, void* dst, const void* src, size_t bytes) {
+  UploadSlot& u = h->up[h->up_next];
+  h->up_next = (h->up_next + 1) % kUploadSlots;
+  if (u.used) AHX_CUDA(h, cudaEventSynchronize(u.ev));
+  if (u.bytes < bytes) {
+    if (u.h) cudaFreeHost(u.h);
+    u.h = nullptr;
+    u.bytes = 0;
+    if (cudaMallocHost(&u.h, bytes) != cudaSuccess) return fail(AHX_ENOMEM, "live solver: pinned allocation failed");
+    u.bytes = bytes;
+  }
+  std::memcpy(u.h, src, bytes);
+  AHX_CUDA(h, cudaMemcpyAsync(dst, u.h, bytes, cudaMemcpyHostToDevice, h->s_step));
+  AHX_CUDA(h, cudaEventRecord(u.ev, h->s_step));
+  u.used = true;
+  return AHX_OK;
+}
+
+ahx_status ensure_dbg(ahx_handle* h) {
+  if (h->d_dbg) return AHX_OK;
+  const size_t bytes = (size_t)h->ps * h->dims.nz * sizeof(float4);
+  if (cudaMalloc(&h->d_dbg, bytes) != cudaSuccess) {
+    h->d_dbg = nullptr;
+    cudaGetLastError();
+    return fail(AHX_ENOMEM, "live solver: debug buffer allocation failed");
+  }
+  AHX_CUDA(h, cudaMemsetAsync(h->d_dbg, 0, bytes, h->s_step));
+  return AHX_OK;
+}
+
+void free_all(ahx_handle* h) {
+  cudaSetDevice(h->dev);
+  if (h->s_step) cudaStreamSynchronize(h->s_step);
+  if (h->s_copy) cudaStreamSynchronize(h->s_copy);
+  for (int p = 0; p < 2; ++p) {
+    if (h->f[p]) cudaFree(h->f[p]);
+    if (h->g[p]) cudaFree(h->g[p]);
+    h->f[p] = h->g[p] = nullptr;
+  }
+  void* devs[] = {h->d_params, h->d_colv, h->d_ktop, h->d_oldk, h->d_dbg, h->d_budget, h->d_stats};
+  for (void* p : devs)
+    if (p) cudaFree(p);
+  h->d_params = nullptr;
+  h->d_colv = nullptr;
+  h->d_ktop = h->d_oldk = nullptr;
+  h->d_dbg = nullptr;
+  h->d_budget = nullptr;
+  h->d_stats = nullptr;
+  for (auto& r : h->reads) {
+    if (r.d_surf) cudaFree(r.d_surf);
+    if (r.d_vol) cudaFree(r.d_vol);
+    if (r.d_tmax) cudaFree(r.d_tmax);
+    if (r.h_surf) cudaFreeHost(r.h_surf);
+    if (r.h_vol) cudaFreeHost(r.h_vol);
+    if (r.h_tmax) cudaFreeHost(r.h_tmax);
+    if (r.ev_kernels) cudaEventDestroy(r.ev_kernels);
+    if (r.ev_done) cudaEventDestroy(r.ev_done);
+    r = ReadSlot{};
+  }
+  for (auto& u : h->up) {
+    if (u.h) cudaFreeHost(u.h);
+    if (u.ev) cudaEventDestroy(u.ev);
+    u = UploadSlot{};
+  }
+  for (auto& f : h->fences) cudaEventDestroy(f.ev);
+  h->fences.clear();
+  if (h->s_step) cudaStreamDestroy(h->s_step);
+  if (h->s_copy) cudaStreamDestroy(h->s_copy);
+  h->s_step = h->s_copy = nullptr;
+}
+
+// bounded wait on an event; the handle lock is not held while waiting
+ahx_status wait_event(ahx_handle* h, cudaEvent_t ev, int timeout_ms) {
+  const auto t0 = std::chrono::steady_clock::now();
+  int spin = 0;
+  for (;;) {
+    const cudaError_t e = cudaEventQuery(ev);
+    if (e == cudaSuccess) return AHX_OK;
+    if (e != cudaErrorNotReady) return cuda_fail(h, e, "cudaEventQuery");
+    if (timeout_ms >= 0) {
+      const auto ms =
+          std::chrono::duration_cast<std::chrono::milliseconds>(std::chrono::steady_clock::now() - t0).count();
+      if (ms >= timeout_ms) return fail(AHX_ETIMEOUT, "live solver: timed out waiting for the GPU");
+    }
+    if (++spin < 200) std::this_thread::yield();
+    else std::this_thread::sleep_for(std::chrono::microseconds(50));
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* ahx_last_error(void) { return g_err.c_str(); }
+
+ahx_status ahx_create(const ahx_dims* dims, ahx_handle** out) {
+  if (!dims || !out) return fail(AHX_EINVAL, "live solver: null argument");
+  *out = nullptr;
+  if (dims->nx < 2 || dims->ny < 2 || dims->nz < 2)
+    return fail(AHX_EINVAL, "live solver: grid must be at least 2 x 2 x 2");
+  const int esize = element_bytes(dims->precision);
+  if (!esize) return fail(AHX_EINVAL, "live solver: unknown precision");
+  if (dims->arith != AHX_ARITH_EXACT && dims->arith != AHX_ARITH_FAST)
+    return fail(AHX_EINVAL, "live solver: unknown arithmetic variant");
+  const int align = 128 / esize;   // x rows start on 128-byte boundaries
+  const int px = (dims->nx + align - 1) / align * align;
+  const uint64_t ps = (uint64_t)px * dims->ny;
+  const uint64_t qs = ps * dims->nz;
+  if (19 * qs >= (1ull << 32))
+    return fail(AHX_EINVAL, "live solver: grid too large for one handle (19 population planes must index in 32 bits)");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return fail(AHX_EDEVICE, "live solver: no CUDA device is available");
+  }
+  int dev = dims->device_ordinal;
+  if (dev < 0) cudaGetDevice(&dev);
+  if (dev >= ndev) return fail(AHX_EINVAL, "live solver: device ordinal out of range");
+  ahx_handle* h = new ahx_handle();
+  h->dev = dev;
+  h->dims = *dims;
+  h->dims.device_ordinal = dev;
+  h->esize = esize;
+  h->px = px;
+  h->ps = (uint32_t)ps;
+  h->qs = (uint32_t)qs;
+  h->zslab = 0;
+  cudaDeviceProp prop;
+  if (cudaSetDevice(dev) != cudaSuccess || cudaGetDeviceProperties(&prop, dev) != cudaSuccess) {
+    delete h;
+    return fail(AHX_EDEVICE, "live solver: cannot use CUDA device");
+  }
+  std::strncpy(h->name, prop.name, sizeof(h->name) - 1);
+  auto bail = [&](ahx_status st, const std::string& m) {
+    free_all(h);
+    delete h;
+    cudaGetLastError();
+    return fail(st, m);
+  };
+  if (cudaStreamCreateWithFlags(&h->s_step, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&h->s_copy, cudaStreamNonBlocking) != cudaSuccess)
+    return bail(AHX_EDEVICE, "live solver: stream creation failed");
+  const size_t fbytes = 19 * qs * esize, gbytes = 7 * qs * esize;
+  const size_t NXY = (size_t)dims->nx * dims->ny;
+  for (int p = 0; p < 2; ++p) {
+    if (cudaMalloc(&h->f[p], fbytes) != cudaSuccess || cudaMalloc(&h->g[p], gbytes) != cudaSuccess)
+      return bail(AHX_ENOMEM, "live solver: buffer allocation failed (out of memory). Try a coarser grid.");
+    cudaMemsetAsync(h->f[p], 0, fbytes, h->s_step);
+    cudaMemsetAsync(h->g[p], 0, gbytes, h->s_step);
+  }
+  if (cudaMalloc(&h->d_params, 64 + 16 * (size_t)dims->nz) != cudaSuccess ||
+      cudaMalloc(&h->d_colv, NXY * sizeof(uint4)) != cudaSuccess ||
+      cudaMalloc(&h->d_ktop, NXY * 4) != cudaSuccess || cudaMalloc(&h->d_oldk, NXY * 4) != cudaSuccess ||
+      cudaMalloc(&h->d_budget, (size_t)kBudgetSlots * kBudgetStride * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&h->d_stats, sizeof(StatsScratch)) != cudaSuccess)
+    return bail(AHX_ENOMEM, "live solver: buffer allocation failed (out of memory)");
+  cudaMemsetAsync(h->d_params, 0, 64 + 16 * (size_t)dims->nz, h->s_step);
+  cudaMemsetAsync(h->d_colv, 0, NXY * sizeof(uint4), h->s_step);
+  cudaMemsetAsync(h->d_ktop, 0, NXY * 4, h->s_step);
+  cudaMemsetAsync(h->d_budget, 0, (size_t)kBudgetSlots * kBudgetStride * sizeof(double), h->s_step);
+  const size_t volw = ((size_t)dims->nz * NXY + 3) / 4;
+  for (auto& r : h->reads) {
+    if (cudaMalloc(&r.d_surf, 3 * NXY * 4) != cudaSuccess || cudaMalloc(&r.d_vol, volw * 4) != cudaSuccess ||
+        cudaMalloc(&r.d_tmax, 4) != cudaSuccess || cudaMallocHost(&r.h_surf, 3 * NXY * 4) != cudaSuccess ||
+        cudaMallocHost(&r.h_vol, volw * 4) != cudaSuccess || cudaMallocHost(&r.h_tmax, 4) != cudaSuccess ||
+        cudaEventCreateWithFlags(&r.ev_kernels, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&r.ev_done, cudaEventDisableTiming) != cudaSuccess)
+      return bail(AHX_ENOMEM, "live solver: read-back buffer allocation failed");
+  }
+  for (auto& u : h->up)
+    if (cudaEventCreateWithFlags(&u.ev, cudaEventDisableTiming) != cudaSuccess)
+      return bail(AHX_EDEVICE, "live solver: event creation failed");
+  if (cudaStreamSynchronize(h->s_step) != cudaSuccess) return bail(AHX_EDEVICE, "live solver: initialisation failed");
+  *out = h;
+  return AHX_OK;
+}
+
+ahx_status ahx_destroy(ahx_handle* h) {
+  if (!h) return fail(AHX_EINVAL, "live solver: null handle");
+  {
+    std::lock_guard<std::mutex> lk(h->mu);
+    if (h->destroyed) return AHX_OK;
+    h->destroyed = true;
+    free_all(h);
+  }
+  // the handle object itself stays allocated so later calls report "destroyed" instead of touching freed memory
+  return AHX_OK;
+}
+
+ahx_status ahx_get_info(ahx_handle* h, ahx_info_out* out) {
+  if (!h || !out) return fail(AHX_EINVAL, "live solver: null argument");
+  std::lock_guard<std::mutex> lk(h->mu);
+  std::memset(out, 0, sizeof(*out));
+  out->nx = h->dims.nx;
+  out->ny = h->dims.ny;
+  out->nz = h->dims.nz;
+  out->px = h->px;
+  out->precision = h->dims.precision;
+  out->arith = h->dims.arith;
+  out->parity = h->parity;
+  out->device_ordinal = h->dev;
+  out->steps = h->steps;
+  out->state_bytes = 2ull * 26ull * h->qs * h->esize;
+  out->bytes_per_cell = 2ull * 26ull * h->esize;
+  std::snprintf(out->device_name, sizeof(out->device_name), "%s", h->name);
+  if (h->destroyed) return fail(AHX_EDESTROYED, "live solver: destroyed");
+  return AHX_OK;
+}
+
+ahx_status ahx_set_params(ahx_handle* h, const void* params, size_t bytes) {
+  if (!h) return fail(AHX_EINVAL, "live solver: null handle");
+  std::lock_guard<std::mutex> lk(h->mu);
+  if (ahx_status st = check(h)) return st;
+  if (!params || bytes != params_bytes(h))
+    return fail(AHX_EINVAL, "live solver: parameter block must be 64 + 16*nz bytes");
+  AHX_CUDA(h, cudaSetDevice(h->dev));
+  return upload(h, h->d_params, params, bytes);
+}
+
+ahx_status ahx_set_columns(ahx_handle* h, const uint32_t* colv) {
+  if (!h) return fail(AHX_EINVAL, "live solver: null handle");
+  std::lock_guard<std::mutex> lk(h->mu);
+  if (ahx_status st = check(h)) return st;
+  if (!colv) return fail(AHX_EINVAL, "live solver: null column records");
+  for (size_t c = 0; c < nxy(h); ++c)
+    if (colv[4 * c] > kMaxLevel || colv[4 * c + 1] > kMaxLevel)
+      return fail(AHX_EINVAL, "live solver: column record with kt or ktop out of range");
+  AHX_CUDA(h, cudaSetDevice(h->dev));
+  return upload(h, h->d_colv, colv, nxy(h) * sizeof(uint4));
+}
+
+ahx_status ahx_set_ktop(ahx_handle* h, const uint32_t* ktop, const uint32_t* old_ktop) {
+  if (!h) return fail(AHX_EINVAL, "live solver: null handle");
+  std::lock_guard<std::mutex> lk(h->mu);
+  if (ahx_status st = check(h)) return st;
+  if (!ktop) return fail(AHX_EINVAL, "live solver: null ktop");
+  for (size_t c = 0; c < nxy(h); ++c)
+    if (ktop[c] > kMaxLevel || (old_ktop && old_ktop[c] > kMaxLevel))
+      return fail(AHX_EINVAL, "live solver: ktop out of range");
+  AHX_CUDA(h, cudaSetDevice(h->dev));
+  if (ahx_status st = upload(h, h->d_ktop, ktop, nxy(h) * 4)) return st;
+  if (old_ktop) {
+    if (ahx_status st = upload(h, h->d_oldk, old_ktop, nxy(h) * 4)) return st;
+    DomainView D = view(h);
+    AHX_CUDA(h, launch_reinit(D, h->dims.precision, h->d_oldk, h->f[h->parity], h->g[h->parity], h->s_step));
+  }
+  return AHX_OK;
+}
+
+ahx_status ahx_init_flow(ahx_handle* h) {
+  if (!h) return fail(AHX_EINVAL, "live solver: null handle");
+  std::lock_guard<std::mutex> lk(h->mu);
+  if (ahx_status st = check(h)) return st;
+  AHX_CUDA(h, cudaSetDevice(h->dev));
+  DomainView D = view(h);
+  AHX_CUDA(h, launch_init(D, h->dims.precision, h->f[0], h->f[1], h->s_step));
+  return AHX_OK;
+}
+
+ahx_status ahx_clear_heat(ahx_handle* h) {
+  if (!h) return fail(AHX_EINVAL, "live solver: null handle");
+  std::lock_guard<std::mutex> lk(h->mu);
+  if (ahx_status st = check(h)) return st;
+  AHX_CUDA(h, cudaSetDevice(h->dev));
+  for (int p = 0; p < 2; ++p) AHX_CUDA(h, cudaMemsetAsync(h->g[p], 0, 7ull * h->qs * h->esize, h->s_step));
+  return AHX_OK;
+}
+
+ahx_status ahx_set_parity(ahx_handle* h, int parity) {
+  if (!h) return fail(AHX_EINVAL, "live solver: null handle");
+  std::lock_guard<std::mutex> lk(h->mu);
+  if (ahx_status st = check(h)) return st;
+  if (parity != 0 && parity != 1) return fail(AHX_EINVAL, "live solver: parity must be 0 or 1");
+  h->parity = parity;
+  return AHX_OK;
+}
+
+ahx_status ahx_step(ahx_handle* h, int n, int mode) {
+  if (!h) return fail(AHX_EINVAL, "live solver: null handle");
+  std::lock_guard<std::mutex> lk(h->mu);
+  if (ahx_status st = check(h)) return st;
+  if (n < 0 || mode < 0 || mode > 2) return fail(AHX_EINVAL, "live solver: bad step count or mode");
+  AHX_CUDA(h, cudaSetDevice(h->dev));
+  if (mode != AHX_MODE_NONE)
+    if (ahx_status st = ensure_dbg(h)) return st;
+  StepLaunch L;
+  L.precision = h->dims.precision;
+  L.budget = h->budget_on;
+  L.block_y = h->block_y;
+  L.zslab = h->zslab;
+  for (int s = 0; s < n; ++s) {
+    L.mode = (mode == AHX_MODE_ACC) ? 2 : ((mode == AHX_MODE_OUT && s == n - 1) ? 1 : 0);
+    DomainView D = view(h);
+    const cudaError_t e = h->dims.arith == AHX_ARITH_FAST ? fast::launch_step(D, L, h->s_step)
+                                                            : exact::launch_step(D, L, h->s_step);
+    if (e != cudaSuccess) return cuda_fail(h, e, "step launch");
+    h->parity ^= 1;
+    ++h->steps;
+  }
+  return AHX_OK;
+}
+
+ahx_status ahx_time_steps(ahx_handle* h, int n, int mode, int timeout_ms, float* ms) {
+  if (!h || !ms) return fail(AHX_EINVAL, "live solver: null argument");
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(h->mu);
+    if (ahx_status st = check(h)) return st;
+    AHX_CUDA(h, cudaSetDevice(h->dev));
+    AHX_CUDA(h, cudaEventCreate(&e0));
+    AHX_CUDA(h, cudaEventCreate(&e1));
+    AHX_CUDA(h, cudaEventRecord(e0, h->s_step));
+  }
+  ahx_status st = ahx_step(h, n, mode);
+  if (st == AHX_OK) {
+    std::lock_guard<std::mutex> lk(h->mu);
+    const cudaError_t e = cudaEventRecord(e1, h->s_step);
+    if (e != cudaSuccess) st = cuda_fail(h, e, "cudaEventRecord");
+  }
+  if (st == AHX_OK) st = wait_event(h, e1, timeout_ms);
+  if (st == AHX_OK) {
+    const cudaError_t e = cudaEventElapsedTime(ms, e0, e1);
+    if (e != cudaSuccess) st = cuda_fail(h, e, "cudaEventElapsedTime");
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return st;
+}
+
+ahx_status ahx_sync(ahx_handle* h, int timeout_ms) {
+  cudaEvent_t ev = nullptr;
+  {
+    if (!h) return fail(AHX_EINVAL, "live solver: null handle");
+    std::lock_guard<std::mutex> lk(h->mu);
+    if (ahx_status st = check(h)) return st;
+    AHX_CUDA(h, cudaSetDevice(h->dev));
+    AHX_CUDA(h, cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    AHX_CUDA(h, cudaEventRecord(ev, h->s_step));
+  }
+  const ahx_status st = wait_event(h, ev, timeout_ms);
+  cudaEventDestroy(ev);
+  return st;
+}
+
+ahx_status ahx_fence(ahx_handle* h, uint64_t* ticket) {
+  if (!h || !ticket) return fail(AHX_EINVAL, "live solver: null argument");
+  std::lock_guard<std::mutex> lk(h->mu);
+  if (ahx_status st = check(h)) return st;
+  AHX_CUDA(h, cudaSetDevice(h->dev));
+  // bound the number of outstanding fences: retire the oldest ones that already passed
+  if (h->fences.size() > 256) {
+    std::vector<Fence> keep;
+    for (auto& f : h->fences) {
+      if (cudaEventQuery(f.ev) == cudaSuccess) cudaEventDestroy(f.ev);
+      else keep.push_back(f);
+    }
+    cudaGetLastError();
+    h->fences.swap(keep);
+  }
+  Fence f;
+  f.ticket = ++h->next_fence;
+  AHX_CUDA(h, cudaEventCreateWithFlags(&f.ev, cudaEventDisableTiming));
+  AHX_CUDA(h, cudaEventRecord(f.ev, h->s_step));
+  h->fences.push_back(f);
+  *ticket = f.ticket;
+  return AHX_OK;
+}
+
+ahx_status ahx_fence_query(ahx_handle* h, uint64_t ticket, int* done) {
+  if (!h || !done) return fail(AHX_EINVAL, "live solver: null argument");
+  std::lock_guard<std::mutex> lk(h->mu);
+  if (ahx_status st = check(h)) return st;
+  *done = 1;   // unknown or retired tickets have passed
+  for (size_t a = 0; a < h->fences.size(); ++a) {
+    if (h->fences[a].ticket != ticket) continue;
+    const cudaError_t e = cudaEventQuery(h->fences[a].ev);
+    if (e == cudaErrorNotReady) {
+      *done = 0;
+    } else if (e != cudaSuccess) {
+      return cuda_fail(h, e, "cudaEventQuery");
+    } else {
+      cudaEventDestroy(h->fences[a].ev);
+      h->fences.erase(h->fences.begin() + a);
+    }
+    break;
+  }
+  return AHX_OK;
+}
+
+ahx_status ahx_read_submit(ahx_handle* h, float conv, float volscale, int nzv, int want_vol, int want_wind,
+                           uint64_t* ticket) {
+  if (!h || !ticket) return fail(AHX_EINVAL, "live solver: null argument");
+  std::lock_guard<std::mutex> lk(h->mu);
+  if (ahx_status st = check(h)) return st;
+  if (nzv < 0 || nzv > h->dims.nz) return fail(AHX_EINVAL, "live solver: nzv out of range");
+  ReadSlot* r = nullptr;
+  for (auto& s : h->reads)
+    if (!s.busy) {
+      r = &s;
+      break;
+    }
+  if (!r) return fail(AHX_EBUSY, "live solver: too many reads in flight");
+  AHX_CUDA(h, cudaSetDevice(h->dev));
+  const size_t NXY = nxy(h);
+  DomainView D = view(h);
+  AHX_CUDA(h, cudaMemsetAsync(r->d_tmax, 0, 4, h->s_step));
+  AHX_CUDA(h, launch_surf(D, h->dims.precision, conv, r->d_surf, h->s_step));
+  AHX_CUDA(h, launch_vol(D, h->dims.precision, nzv, volscale, r->d_vol, r->d_tmax, h->s_step));
+  AHX_CUDA(h, cudaEventRecord(r->ev_kernels, h->s_step));
+  AHX_CUDA(h, cudaStreamWaitEvent(h->s_copy, r->ev_kernels, 0));
+  AHX_CUDA(h, cudaMemcpyAsync(r->h_surf, r->d_surf, (want_wind ? 3 : 1) * NXY * 4, cudaMemcpyDeviceToHost,
+                              h->s_copy));
+  if (want_vol && nzv > 0)
+    AHX_CUDA(h, cudaMemcpyAsync(r->h_vol, r->d_vol, (size_t)nzv * NXY, cudaMemcpyDeviceToHost, h->s_copy));
+  AHX_CUDA(h, cudaMemcpyAsync(r->h_tmax, r->d_tmax, 4, cudaMemcpyDeviceToHost, h->s_copy));
+  AHX_CUDA(h, cudaEventRecord(r->ev_done, h->s_copy));
+  r->busy = true;
+  r->ticket = ++h->next_read;
+  r->nzv = nzv;
+  r->want_vol = want_vol;
+  r->want_wind = want_wind;
+  *ticket = r->ticket;
+  return AHX_OK;
+}
+
+ahx_status ahx_read_wait(ahx_handle* h, uint64_t ticket, int timeout_ms, float* surf, float* u, float* v,
+                         uint8_t* vol, float* theta_max) {
+  if (!h) return fail(AHX_EINVAL, "live solver: null handle");
+  ReadSlot* r = nullptr;
+  cudaEvent_t ev;
+  {
+    std::lock_guard<std::mutex> lk(h->mu);
+    if (h->destroyed) return fail(AHX_EDESTROYED, "live solver: read failed (solver destroyed)");
+    for (auto& s : h->reads)
+      if (s.busy && s.ticket == ticket) r = &s;
+    if (!r) return fail(AHX_EINVAL, "live solver: unknown read ticket");
+    ev = r->ev_done;
+  }
+  if (ahx_status st = wait_event(h, ev, timeout_ms)) return st;
+  std::lock_guard<std::mutex> lk(h->mu);
+  if (h->destroyed) return fail(AHX_EDESTROYED, "live solver: read failed (solver destroyed)");
+  const size_t NXY = nxy(h);
+  if (surf) std::memcpy(surf, r->h_surf, NXY * 4);
+  if (r->want_wind) {
+    if (u) std::memcpy(u, r->h_surf + NXY, NXY * 4);
+    if (v) std::memcpy(v, r->h_surf + 2 * NXY, NXY * 4);
+  }
+  if (vol && r->want_vol) std::memcpy(vol, r->h_vol, (size_t)r->nzv * NXY);
+  if (theta_max) std::memcpy(theta_max, r->h_tmax, 4);
+  r->busy = false;
+  return AHX_OK;
+}
+
+static ahx_status state_io(ahx_handle* h, void* f, void* g, bool is_f64, bool to_host) {
+  AHX_CUDA(h, cudaSetDevice(h->dev));
+  const size_t N = ncells(h);
+  const size_t eb = is_f64 ? 8 : 4;
+  void* stage = nullptr;
+  if (cudaMalloc(&stage, N * eb) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(AHX_ENOMEM, "live solver: staging allocation failed");
+  }
+  DomainView D = view(h);
+  ahx_status st = AHX_OK;
+  for (int pass = 0; pass < 2 && st == AHX_OK; ++pass) {
+    void* host = pass == 0 ? f : g;
+    if (!host) continue;
+    const int nq = pass == 0 ? 19 : 7;
+    void* dev_state = pass == 0 ? h->f[h->parity] : h->g[h->parity];
+    for (int q = 0; q < nq; ++q) {
+      char* hp = static_cast<char*>(host) + (size_t)q * N * eb;
+      cudaError_t e;
+      if (to_host) {
+        e = launch_export_plane(D, h->dims.precision, dev_state, stage, is_f64, q, pass == 1, h->s_step);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(hp, stage, N * eb, cudaMemcpyDeviceToHost, h->s_step);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(h->s_step);
+      } else {
+        e = cudaMemcpyAsync(stage, hp, N * eb, cudaMemcpyHostToDevice, h->s_step);
+        if (e == cudaSuccess)
+          e = launch_import_plane(D, h->dims.precision, stage, is_f64, dev_state, q, pass == 1, h->s_step);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(h->s_step);
+      }
+      if (e != cudaSuccess) {
+        st = cuda_fail(h, e, "state copy");
+        break;
+      }
+    }
+  }
+  cudaFree(stage);
+  return st;
+}
+
+ahx_status ahx_read_state(ahx_handle* h, float* f, float* g) {
+  if (!h) return fail(AHX_EINVAL, "live solver: null handle");
+  std::lock_guard<std::mutex> lk(h->mu);
+  if (ahx_status st = check(h)) return st;
+  return state_io(h, f, g, false, true);
+}
+
+ahx_status ahx_write_state(ahx_handle* h, const float* f, const float* g) {
+  if (!h) return fail(AHX_EINVAL, "live solver: null handle");
+  std::lock_guard<std::mutex> lk(h->mu);
+  if (ahx_status st = check(h)) return st;
+  return state_io(h, const_cast<float*>(f), const_cast<float*>(g), false, false);
+}
+
+ahx_status ahx_read_state_f64(ahx_handle* h, double* f, double* g) {
+  if (!h) return fail(AHX_EINVAL, "live solver: null handle");
+  std::lock_guard<std::mutex> lk(h->mu);
+  if (ahx_status st = check(h)) return st;
+  return state_io(h, f, g, true, true);
+}
+
+ahx_status ahx_write_state_f64(ahx_handle* h, const double* f, const double* g) {
+  if (!h) return fail(AHX_EINVAL, "live solver: null handle");
+  std::lock_guard<std::mutex> lk(h->mu);
+  if (ahx_status st = check(h)) return st;
+  return state_io(h, const_cast<double*>(f), const_cast<double*>(g), true, false);
+}
+
+ahx_status ahx_read_dbg(ahx_handle* h, float* dbg4) {
+  if (!h || !dbg4) return fail(AHX_EINVAL, "live solver: null argument");
+  std::lock_guard<std::mutex> lk(h->mu);
+  if (ahx_status st = check(h)) return st;
+  AHX_CUDA(h, cudaSetDevice(h->dev));
+  if (ahx_status st = ensure_dbg(h)) return st;
+  const size_t rows = (size_t)h->dims.ny * h->dims.nz;
+  AHX_CUDA(h, cudaMemcpy2DAsync(dbg4, (size_t)h->dims.nx * 16, h->d_dbg, (size_t)h->px * 16,
+                                (size_t)h->dims.nx * 16, rows, cudaMemcpyDeviceToHost, h->s_step));
+  AHX_CUDA(h, cudaStreamSynchronize(h->s_step));
+  return AHX_OK;
+}
+
+ahx_status ahx_clear_dbg(ahx_handle* h) {
+  if (!h) return fail(AHX_EINVAL, "live solver: null handle");
+  std::lock_guard<std::mutex> lk(h->mu);
+  if (ahx_status st = check(h)) return st;
+  AHX_CUDA(h, cudaSetDevice(h->dev));
+  if (ahx_status st = ensure_dbg(h)) return st;
+  AHX_CUDA(h, cudaMemsetAsync(h->d_dbg, 0, (size_t)h->ps * h->dims.nz * sizeof(float4), h->s_step));
+  return AHX_OK;
+}
+
+ahx_status ahx_stats(ahx_handle* h, ahx_stats_out* out) {
+  if (!h || !out) return fail(AHX_EINVAL, "live solver: null argument");
+  std::lock_guard<std::mutex> lk(h->mu);
+  if (ahx_status st = check(h)) return st;
+  AHX_CUDA(h, cudaSetDevice(h->dev));
+  AHX_CUDA(h, cudaMemsetAsync(h->d_stats, 0, sizeof(StatsScratch), h->s_step));
+  DomainView D = view(h);
+  AHX_CUDA(h, launch_stats(D, h->dims.precision, h->d_stats, h->s_step));
+  StatsScratch s;
+  AHX_CUDA(h, cudaMemcpyAsync(&s, h->d_stats, sizeof(s), cudaMemcpyDeviceToHost, h->s_step));
+  AHX_CUDA(h, cudaStreamSynchronize(h->s_step));
+  std::memset(out, 0, sizeof(*out));
+  out->sum_theta = s.sum[0];
+  out->sum_ke = s.sum[1];
+  out->sum_rho_dev = s.sum[2];
+  out->count = s.sum[3];
+  std::memcpy(&out->theta_max, &s.tmax_bits, 4);
+  std::memcpy(&out->umax, &s.umax_bits, 4);
+  out->non_finite = s.non_finite;
+  return AHX_OK;
+}
+
+ahx_status ahx_budget_enable(ahx_handle* h, int on) {
+  if (!h) return fail(AHX_EINVAL, "live solver: null handle");
+  std::lock_guard<std::mutex> lk(h->mu);
+  if (ahx_status st = check(h)) return st;
+  h->budget_on = on != 0;
+  return AHX_OK;
+}
+
+ahx_status ahx_budget_read(ahx_handle* h, ahx_budget_out* out, int reset) {
+  if (!h || !out) return fail(AHX_EINVAL, "live solver: null argument");
+  std::lock_guard<std::mutex> lk(h->mu);
+  if (ahx_status st = check(h)) return st;
+  AHX_CUDA(h, cudaSetDevice(h->dev));
+  std::vector<double> b((size_t)kBudgetSlots * kBudgetStride);
+  AHX_CUDA(h, cudaMemcpyAsync(b.data(), h->d_budget, b.size() * sizeof(double), cudaMemcpyDeviceToHost, h->s_step));
+  if (reset) AHX_CUDA(h, cudaMemsetAsync(h->d_budget, 0, b.size() * sizeof(double), h->s_step));
+  AHX_CUDA(h, cudaStreamSynchronize(h->s_step));
+  double acc[11] = {0};
+  for (int s = 0; s < kBudgetSlots; ++s)
+    for (int a = 0; a < 11; ++a) acc[a] += b[(size_t)s * kBudgetStride + a];
+  std::memset(out, 0, sizeof(*out));
+  out->theta_sum = acc[0];
+  out->src_sum = acc[1];
+  for (int a = 0; a < 4; ++a) {
+    out->face_theta_u[a] = acc[2 + a];
+    out->face_u[a] = acc[6 + a];
+  }
+  out->cells = acc[10];
+  return AHX_OK;
+}
+
+ahx_status ahx_set_launch(ahx_handle* h, int block_y, int zslab) {
+  if (!h) return fail(AHX_EINVAL, "live solver: null handle");
+  std::lock_guard<std::mutex> lk(h->mu);
+  if (ahx_status st = check(h)) return st;
+  if (block_y < 0 || block_y > 8 || zslab < 0) return fail(AHX_EINVAL, "live solver: bad launch shape");
+  if (block_y) h->block_y = block_y;
+  if (zslab) h->zslab = zslab;
+  return AHX_OK;
+}
+
+ahx_status ahx_autotune(ahx_handle* h, int steps_per_trial, int* best_block_y, int* best_zslab, float* best_ms) {
+  if (!h) return fail(AHX_EINVAL, "live solver: null handle");
+  std::lock_guard<std::mutex> lk(h->mu);
+  if (ahx_status st = check(h)) return st;
+  if (steps_per_trial < 1) steps_per_trial = 4;
+  AHX_CUDA(h, cudaSetDevice(h->dev));
+  // trials ping-pong between the two state buffers, so they would advance the state: run them on a copy
+  const size_t fbytes = 19ull * h->qs * h->esize, gbytes = 7ull * h->qs * h->esize;
+  void *f0 = nullptr, *f1 = nullptr, *g0 = nullptr, *g1 = nullptr;
+  if (cudaMalloc(&f0, fbytes) != cudaSuccess || cudaMalloc(&f1, fbytes) != cudaSuccess ||
+      cudaMalloc(&g0, gbytes) != cudaSuccess || cudaMalloc(&g1, gbytes) != cudaSuccess) {
+    cudaFree(f0);
+    cudaFree(f1);
+    cudaFree(g0);
+    cudaFree(g1);
+    cudaGetLastError();
+    return fail(AHX_ENOMEM, "live solver: autotune needs a second copy of the state");
+  }
+  AHX_CUDA(h, cudaMemcpyAsync(f0, h->f[h->parity], fbytes, cudaMemcpyDeviceToDevice, h->s_step));
+  AHX_CUDA(h, cudaMemcpyAsync(g0, h->g[h->parity], gbytes, cudaMemcpyDeviceToDevice, h->s_step));
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  const int bys[] = {2, 4, 8};
+  std::vector<int> zss = {h->dims.nz, 32, 16, 8};
+  float best = 1e30f;
+  int bby = h->block_y, bzs = h->zslab;
+  DomainView D = view(h);
+  D.dbg = nullptr;
+  StepLaunch L;
+  L.precision = h->dims.precision;
+  L.mode = 0;
+  L.budget = false;
+  ahx_status st = AHX_OK;
+  for (int by : bys) {
+    for (int zs : zss) {
+      if (zs > h->dims.nz) continue;
+      L.block_y = by;
+      L.zslab = zs;
+      float ms = 0;
+      for (int rep = 0; rep < 2 && st == AHX_OK; ++rep) {   // rep 0 warms up
+        cudaEventRecord(e0, h->s_step);
+        for (int s = 0; s < steps_per_trial; ++s) {
+          D.fA = (s & 1) ? f1 : f0;
+          D.fB = (s & 1) ? f0 : f1;
+          D.gA = (s & 1) ? g1 : g0;
+          D.gB = (s & 1) ? g0 : g1;
+          const cudaError_t e = h->dims.arith == AHX_ARITH_FAST ? fast::launch_step(D, L, h->s_step)
+                                                                  : exact::launch_step(D, L, h->s_step);
+          if (e != cudaSuccess) {
+            st = cuda_fail(h, e, "autotune launch");
+            break;
+          }
+        }
+        cudaEventRecord(e1, h->s_step);
+        cudaEventSynchronize(e1);
+        cudaEventElapsedTime(&ms, e0, e1);
+      }
+      if (st != AHX_OK) break;
+      ms /= steps_per_trial;
+      if (ms < best) {
+        best = ms;
+        bby = by;
+        bzs = zs;
+      }
+    }
+  }
+  cudaStreamSynchronize(h->s_step);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(f0);
+  cudaFree(f1);
+  cudaFree(g0);
+  cudaFree(g1);
+  if (st != AHX_OK) return st;
+  h->block_y = bby;
+  h->zslab = bzs;
+  if (best_block_y) *best_block_y = bby;
+  if (best_zslab) *best_zslab = bzs;
+  if (best_ms) *best_ms = best;
+  return AHX_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,377 @@
+// Satellite kernels of the live solver for sm_100a: near-surface and volume read-back, flow initialisation,
+// solid->fluid re-initialisation, diagnostics, and the layout conversion between the reference's [q][cell] f32
+// layout and the pitched internal storage. Built with -fmad=false like the exact step, so the read-back of the
+// moments is bit-identical to the CPU restatement of the reference kernels.
+#include "fused.cuh"
+#include "launch.h"
+
+namespace ahx {
+
+int element_bytes(int precision) {
+  switch (precision) {
+    case 0: return 4;
+    case 1: return 2;
+    case 2: return 2;
+    case 3: return 8;
+    default: return 0;
+  }
+}
+
+namespace {
+
+__device__ __forceinline__ void load_params_smem(const DomainView& D, ParamsHead& sP, float4* prof) {
+  const int tid = threadIdx.x;
+  if (tid < 16) reinterpret_cast<int*>(&sP)[tid] = reinterpret_cast<const int*>(D.params)[tid];
+  const float4* g = reinterpret_cast<const float4*>(D.params + 64);
+  for (int z = tid; z < D.nz; z += blockDim.x) prof[z] = g[z];
+  __syncthreads();
+}
+
+// genSurfWGSL (kernel.js:435-471): pre-collision theta and force-corrected (u, v)*conv of the first fluid cell of
+// every column, north-up [row][col]; zeros where ktop >= nz.
+template <class S>
+__global__ void __launch_bounds__(128) surf_kernel(DomainView D, float conv, float* sout) {
+  using R = typename Codec<S>::Real;
+  extern __shared__ float4 prof[];
+  __shared__ ParamsHead sP;
+  load_params_smem(D, sP, prof);
+  const int NXY = D.nx * D.ny;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= NXY) return;
+  const int i = c % D.nx, j = c / D.nx;
+  const int o = (D.ny - 1 - j) * D.nx + i;
+  const uint4 cv = __ldg(D.colv + c);
+  const int k = (int)cv.y;
+  if (k < 0 || k >= D.nz) {
+    sout[o] = 0.f;
+    sout[NXY + o] = 0.f;
+    sout[2 * NXY + o] = 0.f;
+    return;
+  }
+  Column<R> C;
+  load_column(D, sP, i, j, C);
+  const uint32_t n = (uint32_t)k * D.ps + (uint32_t)j * (uint32_t)D.px + (uint32_t)i;
+  Cell<R> X;
+  stream_cell<S>(D, sP, prof, C, k, n, X);
+  Macro<R> M;
+  moments_forces<R>(sP, C, k, D.nz, X, M);
+  sout[o] = (float)M.th;
+  sout[NXY + o] = (float)M.ux * conv;
+  sout[2 * NXY + o] = (float)M.uy * conv;
+}
+
+// genVolWGSL (kernel.js:475-520): theta (streamed g, summed) of the lowest nzv levels, north-up [k][row][col],
+// quantised to u8 round(theta*volscale) clamped to 0..255, 4 cells per u32 (little-endian); solid cells are 0; the
+// max theta (>= 0) over these cells into *tmax_bits (f32 bits, non-negative floats order as unsigned).
+template <class S>
+__global__ void __launch_bounds__(256) vol_kernel(DomainView D, int nzv, float volscale, uint32_t* vout,
+                                                  unsigned* tmax_bits) {
+  using R = typename Codec<S>::Real;
+  using K = Codec<S>;
+  __shared__ ParamsHead sP;
+  __shared__ unsigned wmax;
+  const int tid = threadIdx.x;
+  if (tid < 16) reinterpret_cast<int*>(&sP)[tid] = reinterpret_cast<const int*>(D.params)[tid];
+  if (tid == 0) wmax = 0u;
+  __syncthreads();
+  const int nx = D.nx, ny = D.ny, nz = D.nz;
+  const long NXY = (long)nx * ny;
+  const long NVOL = (long)nzv * NXY;
+  const long NW = (NVOL + 3) / 4;
+  const long t = (long)blockIdx.x * blockDim.x + tid;
+  const S* gA = static_cast<const S*>(D.gA);
+  float tmax = 0.f;
+  if (t < NW) {
+    uint32_t packed = 0;
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const long p = 4 * t + e;
+      if (p < NVOL) {
+        const int k = (int)(p / NXY);
+        const long rem = p % NXY;
+        const int i = (int)(rem % nx);
+        const int j = ny - 1 - (int)(rem / nx);
+        const int kg = (int)__ldg(D.ktop + (long)j * nx + i);
+        R th = R(0);
+        if (k >= kg) {
+          const uint32_t n = (uint32_t)k * D.ps + (uint32_t)j * (uint32_t)D.px + (uint32_t)i;
+          R g[7];
+          g[0] = K::dec_g(K::load(gA + n));
+          static_for<6>([&](auto Qm1) {
+            constexpr int q = Qm1 + 1;
+            constexpr int cx = kC7[q][0], cy = kC7[q][1], cz = kC7[q][2];
+            const int si = i - cx, sj = j - cy, sk = k - cz;
+            R gv;
+            if (sk >= nz) {
+              gv = K::dec_g(K::load(gA + (uint32_t)q * D.qs + n));
+            } else if (si < 0 || si >= nx || sj < 0 || sj >= ny) {
+              bool inflow = false;
+              if constexpr (cx == 1) inflow = inflow || (si < 0 && sP.inflow_w != 0);
+              if constexpr (cx == -1) inflow = inflow || (si >= nx && sP.inflow_e != 0);
+              if constexpr (cy == 1) inflow = inflow || (sj < 0 && sP.inflow_s != 0);
+              if constexpr (cy == -1) inflow = inflow || (sj >= ny && sP.inflow_n != 0);
+              gv = inflow ? R(0) : K::dec_g(K::load(gA + (uint32_t)q * D.qs + n));
+            } else if (sk < (int)__ldg(D.ktop + (long)sj * nx + si)) {
+              gv = K::dec_g(K::load(gA + (uint32_t)opp7(q) * D.qs + n));
+            } else {
+              gv = K::dec_g(K::load(gA + (uint32_t)q * D.qs + n - (uint32_t)(cx + cy * D.px + cz * (int)D.ps)));
+            }
+            g[q] = gv;
+          });
+          th = g[0];
+#pragma unroll
+          for (int q = 1; q < 7; ++q) th = th + g[q];
+        }
+        const float thf = (float)th;
+        const float r = rintf(thf * volscale);   // WGSL round(): half to even
+        const uint32_t qv = (uint32_t)fminf(fmaxf(r, 0.f), 255.f);
+        packed |= qv << (8u * (uint32_t)e);
+        tmax = fmaxf(tmax, thf);
+      }
+    }
+    vout[t] = packed;
+  }
+  // block max of the non-negative f32 bits, then one global atomic per block
+  unsigned b = __float_as_uint(fmaxf(tmax, 0.f));
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) b = max(b, __shfl_xor_sync(0xffffffffu, b, o));
+  if ((tid & 31) == 0) atomicMax(&wmax, b);
+  __syncthreads();
+  if (tid == 0 && wmax != 0u) atomicMax(tmax_bits, wmax);
+}
+
+// genInitWGSL (kernel.js:524-553): equilibrium with the inflow profile at the local height above terrain in every
+// cell (solid ones included), written to both population buffers.
+template <class S>
+__global__ void __launch_bounds__(256) init_kernel(DomainView D, S* f0, S* f1) {
+  using R = typename Codec<S>::Real;
+  using K = Codec<S>;
+  const float4* prof = reinterpret_cast<const float4*>(D.params + 64);
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y;
+  const int k = blockIdx.z;
+  if (i >= D.nx) return;
+  const int ktc = (int)__ldg(D.colv + (size_t)j * D.nx + i).x;
+  const int zagl = min(max(k - ktc, 0), D.nz - 1);
+  const float4 pr = __ldg(prof + zagl);
+  const R U = R(pr.x), V = R(pr.y);
+  const R usq = U * U + V * V;
+  const uint32_t n = (uint32_t)k * D.ps + (uint32_t)j * (uint32_t)D.px + (uint32_t)i;
+  static_for<19>([&](auto Q) {
+    constexpr int q = Q;
+    const R cu = R(kC19[q][0]) * U + R(kC19[q][1]) * V;
+    const R fq = R(w19(q)) * (R(1.0) + R(3.0) * cu + R(4.5) * cu * cu - R(1.5) * usq);
+    const S e = K::enc_f(fq, R(w19(q)));
+    f0[(uint32_t)q * D.qs + n] = e;
+    f1[(uint32_t)q * D.qs + n] = e;
+  });
+}
+
+// genReinitWGSL (kernel.js:557-575): cells that turned from solid to fluid (k in [ktop, min(oldk, nz))) get rest
+// equilibrium f = w and theta = 0.
+template <class S>
+__global__ void __launch_bounds__(256) reinit_kernel(DomainView D, const uint32_t* oldk, S* f, S* g) {
+  using R = typename Codec<S>::Real;
+  using K = Codec<S>;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int NXY = D.nx * D.ny;
+  if (c >= NXY) return;
+  const int i = c % D.nx, j = c / D.nx;
+  const int k1 = min((int)oldk[c], D.nz);
+  for (int k = (int)D.ktop[c]; k < k1; ++k) {
+    const uint32_t n = (uint32_t)k * D.ps + (uint32_t)j * (uint32_t)D.px + (uint32_t)i;
+    static_for<19>([&](auto Q) {
+      constexpr int q = Q;
+      f[(uint32_t)q * D.qs + n] = K::enc_f(R(w19(q)), R(w19(q)));
+    });
+    static_for<7>([&](auto Q) {
+      constexpr int q = Q;
+      g[(uint32_t)q * D.qs + n] = K::enc_g(R(0));
+    });
+  }
+}
+
+// genStatsWGSL (kernel.js:580-633) over the fluid cells of the current state: per-cell f32 values (theta,
+// 0.5|j|^2/rho, rho - 1, 1) summed in FP64, max theta (>= 0), non-finite count (rho or theta), max |j|/rho.
+template <class S>
+__global__ void __launch_bounds__(256) stats_kernel(DomainView D, StatsScratch* out) {
+  using R = typename Codec<S>::Real;
+  using K = Codec<S>;
+  const S* fA = static_cast<const S*>(D.fA);
+  const S* gA = static_cast<const S*>(D.gA);
+  const int nx = D.nx, ny = D.ny, nz = D.nz;
+  const long total = (long)nx * ny * nz;
+  double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+  float tmax = 0.f, umax = 0.f;
+  unsigned nonf = 0;
+  for (long c = (long)blockIdx.x * blockDim.x + threadIdx.x; c < total; c += (long)gridDim.x * blockDim.x) {
+    const int i = (int)(c % nx);
+    const int j = (int)((c / nx) % ny);
+    const int k = (int)(c / ((long)nx * ny));
+    if (k < (int)__ldg(D.ktop + (long)j * nx + i)) continue;
+    const uint32_t n = (uint32_t)k * D.ps + (uint32_t)j * (uint32_t)D.px + (uint32_t)i;
+    R f[19];
+    static_for<19>([&](auto Q) {
+      constexpr int q = Q;
+      f[q] = K::dec_f(K::load(fA + (uint32_t)q * D.qs + n), R(w19(q)));
+    });
+    float rho = (float)f[0];
+#pragma unroll
+    for (int q = 1; q < 19; ++q) rho = rho + (float)f[q];
+    auto fq = [&](int q) { return (float)f[q]; };
+    const float jx = moment1<float, 0>(fq), jy = moment1<float, 1>(fq), jz = moment1<float, 2>(fq);
+    float th = (float)K::dec_g(K::load(gA + n));
+#pragma unroll
+    for (int q = 1; q < 7; ++q) th = th + (float)K::dec_g(K::load(gA + (uint32_t)q * D.qs + n));
+    const unsigned br = __float_as_uint(rho) & 0x7f800000u, bt = __float_as_uint(th) & 0x7f800000u;
+    if (br == 0x7f800000u || bt == 0x7f800000u) {
+      ++nonf;
+      continue;
+    }
+    s0 += (double)th;
+    s1 += (double)(0.5f * (jx * jx + jy * jy + jz * jz) / rho);
+    s2 += (double)(rho - 1.0f);
+    s3 += 1.0;
+    tmax = fmaxf(tmax, fmaxf(th, 0.f));
+    umax = fmaxf(umax, sqrtf(jx * jx + jy * jy + jz * jz) / rho);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+    s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+    s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+    s3 += __shfl_xor_sync(0xffffffffu, s3, o);
+    tmax = fmaxf(tmax, __shfl_xor_sync(0xffffffffu, tmax, o));
+    umax = fmaxf(umax, __shfl_xor_sync(0xffffffffu, umax, o));
+    nonf += __shfl_xor_sync(0xffffffffu, nonf, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (s3 != 0.0 || s0 != 0.0) {
+      atomicAdd(&out->sum[0], s0);
+      atomicAdd(&out->sum[1], s1);
+      atomicAdd(&out->sum[2], s2);
+      atomicAdd(&out->sum[3], s3);
+    }
+    atomicMax(&out->tmax_bits, __float_as_uint(tmax));
+    atomicMax(&out->umax_bits, __float_as_uint(umax));
+    if (nonf) atomicAdd(&out->non_finite, nonf);
+  }
+}
+
+// reference plane [cell] (f32 or f64) <-> internal pitched plane q
+template <class S>
+__global__ void __launch_bounds__(256) import_plane_kernel(DomainView D, const void* ref, int ref_is_f64, S* dst,
+                                                           int q, int is_g) {
+  using R = typename Codec<S>::Real;
+  using K = Codec<S>;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y, k = blockIdx.z;
+  if (i >= D.nx) return;
+  const size_t c = ((size_t)k * D.ny + j) * D.nx + i;
+  const R v = ref_is_f64 ? R(static_cast<const double*>(ref)[c]) : R(static_cast<const float*>(ref)[c]);
+  const double w = q == 0 ? 1.0 / 3 : (q < 7 ? 1.0 / 18 : 1.0 / 36);
+  const uint32_t n = (uint32_t)k * D.ps + (uint32_t)j * (uint32_t)D.px + (uint32_t)i;
+  dst[(uint32_t)q * D.qs + n] = is_g ? K::enc_g(v) : K::enc_f(v, R(w));
+}
+
+template <class S>
+__global__ void __launch_bounds__(256) export_plane_kernel(DomainView D, const S* src, void* ref, int ref_is_f64,
+                                                           int q, int is_g) {
+  using R = typename Codec<S>::Real;
+  using K = Codec<S>;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y, k = blockIdx.z;
+  if (i >= D.nx) return;
+  const size_t c = ((size_t)k * D.ny + j) * D.nx + i;
+  const double w = q == 0 ? 1.0 / 3 : (q < 7 ? 1.0 / 18 : 1.0 / 36);
+  const uint32_t n = (uint32_t)k * D.ps + (uint32_t)j * (uint32_t)D.px + (uint32_t)i;
+  const S e = src[(uint32_t)q * D.qs + n];
+  const R v = is_g ? K::dec_g(e) : K::dec_f(e, R(w));
+  if (ref_is_f64) static_cast<double*>(ref)[c] = (double)v;
+  else static_cast<float*>(ref)[c] = (float)v;
+}
+
+template <class F>
+cudaError_t dispatch(int precision, F&& f) {
+  switch (precision) {
+    case 0: return f(float{});
+    case 1: return f(__half{});
+    case 2: return f(__nv_bfloat16{});
+    case 3: return f(double{});
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+}  // namespace
+
+cudaError_t launch_init(const DomainView& D, int precision, void* f0, void* f1, cudaStream_t s) {
+  return dispatch(precision, [&](auto tag) {
+    using S = decltype(tag);
+    dim3 grid((D.nx + 255) / 256, D.ny, D.nz);
+    init_kernel<S><<<grid, 256, 0, s>>>(D, static_cast<S*>(f0), static_cast<S*>(f1));
+    return cudaGetLastError();
+  });
+}
+
+cudaError_t launch_reinit(const DomainView& D, int precision, const uint32_t* oldk, void* f, void* g,
+                          cudaStream_t s) {
+  return dispatch(precision, [&](auto tag) {
+    using S = decltype(tag);
+    const int NXY = D.nx * D.ny;
+    reinit_kernel<S><<<(NXY + 255) / 256, 256, 0, s>>>(D, oldk, static_cast<S*>(f), static_cast<S*>(g));
+    return cudaGetLastError();
+  });
+}
+
+cudaError_t launch_surf(const DomainView& D, int precision, float conv, float* sout, cudaStream_t s) {
+  return dispatch(precision, [&](auto tag) {
+    using S = decltype(tag);
+    const int NXY = D.nx * D.ny;
+    surf_kernel<S><<<(NXY + 127) / 128, 128, (size_t)D.nz * sizeof(float4), s>>>(D, conv, sout);
+    return cudaGetLastError();
+  });
+}
+
+cudaError_t launch_vol(const DomainView& D, int precision, int nzv, float volscale, uint32_t* vout,
+                       unsigned* tmax_bits, cudaStream_t s) {
+  return dispatch(precision, [&](auto tag) {
+    using S = decltype(tag);
+    const long NW = ((long)nzv * D.nx * D.ny + 3) / 4;
+    if (NW == 0) return cudaSuccess;
+    vol_kernel<S><<<(unsigned)((NW + 255) / 256), 256, 0, s>>>(D, nzv, volscale, vout, tmax_bits);
+    return cudaGetLastError();
+  });
+}
+
+cudaError_t launch_stats(const DomainView& D, int precision, StatsScratch* out, cudaStream_t s) {
+  return dispatch(precision, [&](auto tag) {
+    using S = decltype(tag);
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    stats_kernel<S><<<sms * 8, 256, 0, s>>>(D, out);
+    return cudaGetLastError();
+  });
+}
+
+cudaError_t launch_import_plane(const DomainView& D, int precision, const void* ref_plane, int ref_is_f64, void* dst,
+                                int q, int is_g, cudaStream_t s) {
+  return dispatch(precision, [&](auto tag) {
+    using S = decltype(tag);
+    dim3 grid((D.nx + 255) / 256, D.ny, D.nz);
+    import_plane_kernel<S><<<grid, 256, 0, s>>>(D, ref_plane, ref_is_f64, static_cast<S*>(dst), q, is_g);
+    return cudaGetLastError();
+  });
+}
+
+cudaError_t launch_export_plane(const DomainView& D, int precision, const void* src, void* ref_plane, int ref_is_f64,
+                                int q, int is_g, cudaStream_t s) {
+  return dispatch(precision, [&](auto tag) {
+    using S = decltype(tag);
+    dim3 grid((D.nx + 255) / 256, D.ny, D.nz);
+    export_plane_kernel<S><<<grid, 256, 0, s>>>(D, static_cast<const S*>(src), ref_plane, ref_is_f64, q, is_g);
+    return cudaGetLastError();
+  });
+}
+
+}  // namespace ahx

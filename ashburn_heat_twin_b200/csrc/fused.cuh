@@ -1,0 +1,487 @@
+// The fused D3Q19 + D3Q7 stream-collide step of the live solver for sm_100a, and the pre-collision moment
+// extraction the near-surface read-back uses.
+//
+// Algorithm: js/live/kernel.js of the reference, genStepWGSL (kernel.js:395-431) with its sections secProfile
+// (:112-120), secNeighbourCache (:102-110), secOutflowPrelude (:122-148), secStreamF (:159-217), secStreamG
+// (:219-243), secMoments (:264-277), secForces (:279-306), secRelax (:308-338), secCollision (:340-367),
+// secScalarCollision (:369-386). Every floating-point expression keeps the reference's operand order; compiled with
+// -fmad=false the result is the reference arithmetic with IEEE-rounded f32 operations.
+//
+// B200 mapping (not the reference's one-thread-per-cell linear dispatch):
+//   * one thread per (i, j) column walking a z-slab [k0, k1): the column record, the 3x3 neighbour ktop cache, the
+//     face flags and the outflow-sponge term are loaded / computed once per column instead of once per cell, and
+//     solid cells below ktop are skipped without a launch slot;
+//   * a warp is 32 consecutive i of one row, rows are 128-byte aligned (pitch px), so each population plane is read
+//     and written as full 128-byte lines (the +-1 x shifts of the pull touch one extra sector, served by L1/L2);
+//   * the boundary rules of the stream become an index remap: every population is one unconditional load from
+//     (source plane, source cell) where bounce-back and the free-slip lid only change the plane and the cell; the
+//     in/outflow faces (a thin set of columns) patch the loaded own value afterwards. So all 26 loads of a cell are
+//     independent and in flight together;
+//   * reads use the non-coherent path (the source buffer is read-only during a step), writes are streaming stores.
+#pragma once
+
+#include "lattice.cuh"
+
+namespace ahx {
+
+template <class R, int cx, int cy, int cz>
+__device__ __forceinline__ R cdot(R a, R b, R c) {
+  // (cx)*a + (cy)*b + (cz)*c over the nonzero components, x y z order; 0 if none (kernel.js:184-199, 342-345)
+  R acc = R(0);
+  bool first = true;
+  if constexpr (cx != 0) { acc = R(cx) * a; first = false; }
+  if constexpr (cy != 0) { acc = first ? R(cy) * b : acc + R(cy) * b; first = false; }
+  if constexpr (cz != 0) { acc = first ? R(cz) * c : acc + R(cz) * c; first = false; }
+  (void)first;
+  return acc;
+}
+
+// signed sum over q of the values whose c[comp] is +-1, in q order (kernel.js:245-252)
+template <class R, int comp, class F>
+__device__ __forceinline__ R moment1(const F& fq) {
+  R acc = R(0);
+  bool first = true;
+  static_for<19>([&](auto Q) {
+    constexpr int q = Q;
+    constexpr int c = kC19[q][comp];
+    if constexpr (c != 0) {
+      const R v = fq(q);
+      if (first) acc = (c > 0) ? v : -v;
+      else acc = (c > 0) ? acc + v : acc - v;
+      first = false;
+    }
+  });
+  return acc;
+}
+
+// second moment Pi_pr in q order (kernel.js:254-262)
+template <class R, int p, int r>
+__device__ __forceinline__ R moment2(const R* f) {
+  R acc = R(0);
+  bool first = true;
+  static_for<19>([&](auto Q) {
+    constexpr int q = Q;
+    constexpr int v = kC19[q][p] * kC19[q][r];
+    if constexpr (v != 0) {
+      if (first) acc = (v > 0) ? f[q] : -f[q];
+      else acc = (v > 0) ? acc + f[q] : acc - f[q];
+      first = false;
+    }
+  });
+  return acc;
+}
+
+// Everything a column needs that does not depend on k.
+template <class R>
+struct Column {
+  int i, j, ktc, kg;
+  float cd, qsrc;
+  int kn[3][3];          // ktop of the 3x3 neighbourhood, clamped at the edges (kernel.js:102-110)
+  bool latW, latE, latS, latN;   // this column lies on the west / east / south / north face
+  bool onb;              // on an outflow face: needs the outflow prelude (kernel.js:125)
+  bool face;             // on any lateral face: some sources are outside the domain
+  bool spon;             // inside the outflow viscous sponge (kernel.js:322-330)
+  R spg;                 // 0.15*rr*rr of the sponge
+};
+
+template <class R>
+__device__ __forceinline__ void load_column(const DomainView& D, const ParamsHead& P, int i, int j, Column<R>& C) {
+  const int nx = D.nx, ny = D.ny;
+  const uint4 cv = __ldg(D.colv + (size_t)j * nx + i);
+  C.i = i;
+  C.j = j;
+  C.ktc = (int)cv.x;
+  C.kg = (int)cv.y;
+  C.cd = __uint_as_float(cv.z);
+  C.qsrc = __uint_as_float(cv.w);
+  const int im = max(i - 1, 0), ip = min(i + 1, nx - 1), jm = max(j - 1, 0), jp = min(j + 1, ny - 1);
+  const int xs[3] = {im, i, ip}, ys[3] = {jm, j, jp};
+#pragma unroll
+  for (int ox = 0; ox < 3; ++ox)
+#pragma unroll
+    for (int oy = 0; oy < 3; ++oy)
+      C.kn[ox][oy] = (ox == 1 && oy == 1) ? C.kg : (int)__ldg(D.ktop + (size_t)ys[oy] * nx + xs[ox]);
+  C.latW = (i == 0);
+  C.latE = (i == nx - 1);
+  C.latS = (j == 0);
+  C.latN = (j == ny - 1);
+  C.face = C.latW || C.latE || C.latS || C.latN;
+  C.onb = (C.latW && P.inflow_w == 0) || (C.latE && P.inflow_e == 0) || (C.latS && P.inflow_s == 0) ||
+          (C.latN && P.inflow_n == 0);
+  int dmin = 1000;
+  if (P.inflow_w == 0 && i < dmin) dmin = i;
+  if (P.inflow_e == 0 && nx - 1 - i < dmin) dmin = nx - 1 - i;
+  if (P.inflow_s == 0 && j < dmin) dmin = j;
+  if (P.inflow_n == 0 && ny - 1 - j < dmin) dmin = ny - 1 - j;
+  C.spon = dmin < P.nsw;
+  C.spg = R(0);
+  if (C.spon) {
+    const R rr = (R(P.nsw) - R(dmin)) / R(P.nsw);
+    C.spg = R(0.15) * rr * rr;
+  }
+}
+
+// is the source of direction (cx, cy) outside the domain for this column (kernel.js:166-167)
+template <int cx, int cy, class R>
+__device__ __forceinline__ bool lateral_out(const Column<R>& C) {
+  bool r = false;
+  if constexpr (cx == 1) r = r || C.latW;
+  if constexpr (cx == -1) r = r || C.latE;
+  if constexpr (cy == 1) r = r || C.latS;
+  if constexpr (cy == -1) r = r || C.latN;
+  return r;
+}
+
+// inflowCond (kernel.js:150-157), given that the source is outside
+template <int cx, int cy, class R>
+__device__ __forceinline__ bool inflow_cond(const Column<R>& C, const ParamsHead& P) {
+  bool r = false;
+  if constexpr (cx == 1) r = r || (C.latW && P.inflow_w != 0);
+  if constexpr (cx == -1) r = r || (C.latE && P.inflow_e != 0);
+  if constexpr (cy == 1) r = r || (C.latS && P.inflow_s != 0);
+  if constexpr (cy == -1) r = r || (C.latN && P.inflow_n != 0);
+  return r;
+}
+
+// Pre-collision state of one cell: the streamed populations plus the profile values used later.
+template <class R>
+struct Cell {
+  R f[19], g[7];
+  R uI, vI, kb;
+};
+
+// secProfile + secOutflowPrelude + secStreamF + secStreamG for cell (C.i, C.j, k); n is the pitched cell index.
+template <class S>
+__device__ __forceinline__ void stream_cell(const DomainView& D, const ParamsHead& P, const float4* prof,
+                                            const Column<typename Codec<S>::Real>& C, int k, uint32_t n,
+                                            Cell<typename Codec<S>::Real>& X) {
+  using R = typename Codec<S>::Real;
+  using K = Codec<S>;
+  const S* fA = static_cast<const S*>(D.fA);
+  const S* gA = static_cast<const S*>(D.gA);
+  const uint32_t qs = D.qs, ps = D.ps, px = (uint32_t)D.px;
+  const bool top = (k == D.nz - 1);
+  // secProfile
+  int zagl = k - C.ktc;
+  if (zagl < 0) zagl = 0;
+  if (zagl > D.nz - 1) zagl = D.nz - 1;   // unreachable for valid columns (kt >= 1); keeps the index in bounds
+  const float4 pr = prof[zagl];
+  const R uI = R(pr.x), vI = R(pr.y);
+  X.uI = uI;
+  X.vI = vI;
+  X.kb = R(pr.z);
+
+  // secStreamF / secStreamG as an index remap: one load per population
+  X.f[0] = K::dec_f(K::load(fA + n), R(w19(0)));
+  static_for<18>([&](auto Qm1) {
+    constexpr int q = Qm1 + 1;
+    constexpr int cx = kC19[q][0], cy = kC19[q][1], cz = kC19[q][2];
+    const int sk = k - cz;
+    const bool lat = lateral_out<cx, cy>(C);
+    uint32_t off;
+    if (cz == -1 && top) {
+      // free-slip lid: the z-mirrored population from the same layer, or the own cell's when the lateral source
+      // is outside or solid (kernel.js:168-181)
+      constexpr int m = mirz19(q);
+      const bool own = lat || (k < C.kn[1 - cx][1 - cy]);
+      off = (uint32_t)m * qs + (own ? n : n - (uint32_t)(cx + cy * (int)px));
+    } else if (lat) {
+      off = (uint32_t)q * qs + n;   // in/outflow: patched below from the own value
+    } else if (sk < C.kn[1 - cx][1 - cy]) {
+      off = (uint32_t)opp19(q) * qs + n;   // half-way bounce-back (kernel.js:209-210)
+    } else {
+      off = (uint32_t)q * qs + n - (uint32_t)(cx + cy * (int)px + cz * (int)ps);
+    }
+    X.f[q] = K::dec_f(K::load(fA + off), R(w19(q)));
+  });
+  X.g[0] = K::dec_g(K::load(gA + n));
+  static_for<6>([&](auto Qm1) {
+    constexpr int q = Qm1 + 1;
+    constexpr int cx = kC7[q][0], cy = kC7[q][1], cz = kC7[q][2];
+    const int sk = k - cz;
+    const bool lat = lateral_out<cx, cy>(C);
+    uint32_t off;
+    if ((cz == -1 && top) || lat) {
+      off = (uint32_t)q * qs + n;   // zero-gradient lid / outflow: own value; inflow patched to 0 below
+    } else if (sk < C.kn[1 - cx][1 - cy]) {
+      off = (uint32_t)opp7(q) * qs + n;
+    } else {
+      off = (uint32_t)q * qs + n - (uint32_t)(cx + cy * (int)px + cz * (int)ps);
+    }
+    X.g[q] = K::dec_g(K::load(gA + off));
+  });
+
+  if (C.face) {
+    // secOutflowPrelude (kernel.js:122-148): own-cell density and velocity on outflow faces
+    R rn = R(1), uxn = R(0), uyn = R(0), uzn = R(0);
+    if (C.onb) {
+      R own[19];
+      static_for<19>([&](auto Q) {
+        constexpr int q = Q;
+        own[q] = K::dec_f(K::load(fA + (uint32_t)q * qs + n), R(w19(q)));
+      });
+      rn = own[0];
+#pragma unroll
+      for (int q = 1; q < 19; ++q) rn = rn + own[q];
+      auto fo = [&](int q) { return own[q]; };
+      uxn = moment1<R, 0>(fo) / rn;
+      uyn = moment1<R, 1>(fo) / rn;
+      uzn = moment1<R, 2>(fo) / rn;
+    }
+    const R usqn = uxn * uxn + uyn * uyn + uzn * uzn;
+    R uxc = uxn, uyc = uyn;
+    if (P.oclip != 0) {
+      if (C.latW && P.inflow_w == 0 && uxc > R(0)) uxc = R(0);
+      if (C.latE && P.inflow_e == 0 && uxc < R(0)) uxc = R(0);
+      if (C.latS && P.inflow_s == 0 && uyc > R(0)) uyc = R(0);
+      if (C.latN && P.inflow_n == 0 && uyc < R(0)) uyc = R(0);
+    }
+    const R usqc = uxc * uxc + uyc * uyc + uzn * uzn;
+    static_for<18>([&](auto Qm1) {
+      constexpr int q = Qm1 + 1;
+      constexpr int cx = kC19[q][0], cy = kC19[q][1], cz = kC19[q][2];
+      if constexpr (cx != 0 || cy != 0) {
+        if (!(cz == -1 && top) && lateral_out<cx, cy>(C)) {
+          const R w = R(w19(q));
+          if (inflow_cond<cx, cy>(C, P)) {
+            const R cu = cdot<R, cx, cy, 0>(uI, vI, R(0));
+            X.f[q] = w * (R(1.0) + R(3.0) * cu + R(4.5) * cu * cu - R(1.5) * (uI * uI + vI * vI));
+          } else {
+            const R cu = cdot<R, cx, cy, cz>(uxn, uyn, uzn);
+            if (P.oclip != 0) {
+              const R cuc = cdot<R, cx, cy, cz>(uxc, uyc, uzn);
+              X.f[q] = X.f[q] + w * ((R(1.0) + R(3.0) * cuc + R(4.5) * cuc * cuc - R(1.5) * usqc) -
+                                     rn * (R(1.0) + R(3.0) * cu + R(4.5) * cu * cu - R(1.5) * usqn));
+            } else {
+              X.f[q] = X.f[q] + w * (R(1.0) - rn) * (R(1.0) + R(3.0) * cu + R(4.5) * cu * cu - R(1.5) * usqn);
+            }
+          }
+        }
+      }
+    });
+    static_for<6>([&](auto Qm1) {
+      constexpr int q = Qm1 + 1;
+      constexpr int cx = kC7[q][0], cy = kC7[q][1], cz = kC7[q][2];
+      if constexpr (cx != 0 || cy != 0) {
+        if (!(cz == -1 && top) && lateral_out<cx, cy>(C) && inflow_cond<cx, cy>(C, P)) X.g[q] = R(0);
+      }
+    });
+  }
+}
+
+template <class R>
+struct Macro {
+  R rho, jx, jy, jz, th;
+  R Fx, Fy, Fz, sg, ux, uy, uz;
+};
+
+// secMoments (first moments only) + secForces (kernel.js:264-306)
+template <class R>
+__device__ __forceinline__ void moments_forces(const ParamsHead& P, const Column<R>& C, int k, int nz,
+                                               const Cell<R>& X, Macro<R>& M) {
+  R rho = X.f[0];
+#pragma unroll
+  for (int q = 1; q < 19; ++q) rho = rho + X.f[q];
+  auto fq = [&](int q) { return X.f[q]; };
+  const R jx = moment1<R, 0>(fq), jy = moment1<R, 1>(fq), jz = moment1<R, 2>(fq);
+  R th = X.g[0];
+#pragma unroll
+  for (int q = 1; q < 7; ++q) th = th + X.g[q];
+  R Fx = R(0), Fy = R(0);
+  R Fz = rho * R(P.gbeta) * th;
+  if (k == C.kg && C.kg == C.ktc) {
+    // log-law drag in the first fluid cell of building-free columns, limited so it never reverses the flow
+    const R cd = R(C.cd);
+    const R ux0 = jx / rho, uy0 = jy / rho;
+    const R sp = sqrt(ux0 * ux0 + uy0 * uy0);
+    Fx = -rho * cd * sp * ux0;
+    Fy = -rho * cd * sp * uy0;
+    const R lim = R(0.5) * rho;
+    if (cd * sp > R(0.5)) {
+      Fx = -lim * ux0;
+      Fy = -lim * uy0;
+    }
+  }
+  R sg = R(0);
+  if (k >= nz - P.nsp) {
+    // top sponge: relax u toward the inflow profile, damp uz
+    const R aa = (R(k - (nz - P.nsp)) + R(1.0)) / R(P.nsp);
+    sg = R(P.sigmax) * aa * aa;
+    Fx += rho * sg * (X.uI - jx / rho);
+    Fy += rho * sg * (X.vI - jy / rho);
+    Fz += -rho * sg * (jz / rho);
+  }
+  M.rho = rho;
+  M.jx = jx;
+  M.jy = jy;
+  M.jz = jz;
+  M.th = th;
+  M.Fx = Fx;
+  M.Fy = Fy;
+  M.Fz = Fz;
+  M.sg = sg;
+  M.ux = (jx + R(0.5) * Fx) / rho;
+  M.uy = (jy + R(0.5) * Fy) / rho;
+  M.uz = (jz + R(0.5) * Fz) / rho;
+}
+
+// secRelax + secCollision + secScalarCollision (kernel.js:308-386); writes the next state of cell n
+template <class S>
+__device__ __forceinline__ void collide_store(const DomainView& D, const ParamsHead& P,
+                                              const Column<typename Codec<S>::Real>& C, int k, uint32_t n,
+                                              const Cell<typename Codec<S>::Real>& X,
+                                              const Macro<typename Codec<S>::Real>& M) {
+  using R = typename Codec<S>::Real;
+  using K = Codec<S>;
+  S* fB = static_cast<S*>(D.fB);
+  S* gB = static_cast<S*>(D.gB);
+  const uint32_t qs = D.qs;
+  const R rho = M.rho, ux = M.ux, uy = M.uy, uz = M.uz, Fx = M.Fx, Fy = M.Fy, Fz = M.Fz;
+  const R* f = X.f;
+  const R Pxx = moment2<R, 0, 0>(f), Pyy = moment2<R, 1, 1>(f), Pzz = moment2<R, 2, 2>(f);
+  const R Pxy = moment2<R, 0, 1>(f), Pxz = moment2<R, 0, 2>(f), Pyz = moment2<R, 1, 2>(f);
+  const R usq = ux * ux + uy * uy + uz * uz;
+  const R r3 = rho * R(1.0 / 3.0);
+  const R Nxx = Pxx - r3 - rho * ux * ux;
+  const R Nyy = Pyy - r3 - rho * uy * uy;
+  const R Nzz = Pzz - r3 - rho * uz * uz;
+  const R Nxy = Pxy - rho * ux * uy;
+  const R Nxz = Pxz - rho * ux * uz;
+  const R Nyz = Pyz - rho * uy * uz;
+  const R Pn = sqrt(Nxx * Nxx + Nyy * Nyy + Nzz * Nzz + R(2.0) * (Nxy * Nxy + Nxz * Nxz + Nyz * Nyz));
+  const R kb = X.kb;
+  R tb = R(P.tau0) + R(3.0) * R(P.momfac) * kb;
+  if (C.spon) tb += C.spg;
+  const R tau = R(0.5) * (tb + sqrt(tb * tb + R(P.cs2smag) * Pn / rho));
+  const R nusgs = (tau - tb) * R(1.0 / 3.0);
+  const R kap = nusgs / R(P.prt) + kb + R(P.kfloor);
+  const R taug = R(0.5) + R(4.0) * kap;
+  const R om = R(1.0) - R(1.0) / tau;
+  const R fpre = R(1.0) - R(0.5) / tau;
+  const R trN = (Nxx + Nyy + Nzz) * R(1.0 / 3.0);
+  const R uF = ux * Fx + uy * Fy + uz * Fz;
+  static_for<19>([&](auto Q) {
+    constexpr int q = Q;
+    constexpr int cx = kC19[q][0], cy = kC19[q][1], cz = kC19[q][2];
+    const R w = R(w19(q));
+    const R w45 = R(4.5 * w19(q));
+    const R cu = cdot<R, cx, cy, cz>(ux, uy, uz);
+    const R feq = w * rho * (R(1.0) + R(3.0) * cu + R(4.5) * cu * cu - R(1.5) * usq);
+    R qn = R(0);
+    bool first = true;
+    auto addq = [&](R v) {
+      qn = first ? v : qn + v;
+      first = false;
+    };
+    if constexpr (cx != 0) addq(Nxx);
+    if constexpr (cy != 0) addq(Nyy);
+    if constexpr (cz != 0) addq(Nzz);
+    if constexpr (cx != 0 && cy != 0) addq(R(2.0) * R(cx * cy) * Nxy);
+    if constexpr (cx != 0 && cz != 0) addq(R(2.0) * R(cx * cz) * Nxz);
+    if constexpr (cy != 0 && cz != 0) addq(R(2.0) * R(cy * cz) * Nyz);
+    const R fr = w45 * (qn - trN);
+    const R cF = cdot<R, cx, cy, cz>(Fx, Fy, Fz);
+    const R Fq = fpre * w * (R(3.0) * (cF - uF) + R(9.0) * cu * cF);
+    __stcs(fB + (uint32_t)q * qs + n, K::enc_f(feq + om * fr + Fq, w));
+  });
+  R Ssrc = R(0);
+  if (k == C.kg) Ssrc = R(C.qsrc) * R(P.srcscale);
+  const R omg = R(1.0) / taug;
+  static_for<7>([&](auto Q) {
+    constexpr int q = Q;
+    constexpr int cx = kC7[q][0], cy = kC7[q][1], cz = kC7[q][2];
+    const R w = R(w7(q));
+    const R geq = w * M.th * (R(1.0) + R(4.0) * cdot<R, cx, cy, cz>(ux, uy, uz));
+    __stcs(gB + (uint32_t)q * qs + n, K::enc_g((X.g[q] + omg * (geq - X.g[q]) + w * Ssrc) * (R(1.0) - M.sg)));
+  });
+}
+
+// Budget accumulators of one thread (summed over its cells, then reduced per block into FP64).
+struct BudgetAcc {
+  float theta, src, cells;
+  float ftu[4], fu[4];
+};
+
+constexpr int kBlockX = 32;
+
+// The fused step over one z-slab of the columns of a block. MODE: 0 none, 1 write dbg, 2 accumulate dbg.
+template <class S, int MODE, bool BUDGET>
+__device__ __forceinline__ void step_block(const DomainView& D, int bx, int by, int bz, int zslab) {
+  using R = typename Codec<S>::Real;
+  extern __shared__ float4 smem_prof[];
+  __shared__ ParamsHead sP;
+  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+  const int nthr = blockDim.x * blockDim.y;
+  if (tid < 16) reinterpret_cast<int*>(&sP)[tid] = reinterpret_cast<const int*>(D.params)[tid];
+  const float4* gprof = reinterpret_cast<const float4*>(D.params + 64);
+  for (int z = tid; z < D.nz; z += nthr) smem_prof[z] = gprof[z];
+  __syncthreads();
+  const ParamsHead& P = sP;
+
+  const int i = bx * kBlockX + threadIdx.x;
+  const int j = by * blockDim.y + threadIdx.y;
+  const int k0 = bz * zslab;
+  const int k1 = min(D.nz, k0 + zslab);
+  BudgetAcc B;
+  if constexpr (BUDGET) {
+    B.theta = B.src = B.cells = 0.f;
+#pragma unroll
+    for (int a = 0; a < 4; ++a) B.ftu[a] = B.fu[a] = 0.f;
+  }
+  if (i < D.nx && j < D.ny) {
+    Column<R> C;
+    load_column(D, P, i, j, C);
+    const uint32_t base = (uint32_t)j * (uint32_t)D.px + (uint32_t)i;
+    for (int k = max(k0, C.kg); k < k1; ++k) {
+      const uint32_t n = (uint32_t)k * D.ps + base;
+      Cell<R> X;
+      stream_cell<S>(D, P, smem_prof, C, k, n, X);
+      Macro<R> M;
+      moments_forces<R>(P, C, k, D.nz, X, M);
+      collide_store<S>(D, P, C, k, n, X, M);
+      if constexpr (MODE == 1) {
+        D.dbg[n] = make_float4((float)M.th, (float)M.ux, (float)M.uy, (float)M.uz);
+      } else if constexpr (MODE == 2) {
+        float4 a = D.dbg[n];
+        a.x = a.x + (float)M.th;
+        a.y = a.y + (float)M.ux;
+        a.z = a.z + (float)M.uy;
+        a.w = a.w + (float)M.uz;
+        D.dbg[n] = a;
+      }
+      if constexpr (BUDGET) {
+        const float th = (float)M.th, ux = (float)M.ux, uy = (float)M.uy;
+        B.theta += th;
+        B.cells += 1.f;
+        if (k == C.kg) B.src += C.qsrc * P.srcscale;
+        if (C.latW) { B.ftu[0] += th * ux; B.fu[0] += ux; }
+        if (C.latE) { B.ftu[1] += th * ux; B.fu[1] += ux; }
+        if (C.latS) { B.ftu[2] += th * uy; B.fu[2] += uy; }
+        if (C.latN) { B.ftu[3] += th * uy; B.fu[3] += uy; }
+      }
+    }
+  }
+  if constexpr (BUDGET) {
+    // warp shuffle in FP64, then shared-memory FP64 atomics per block, then one global FP64 atomic per block and
+    // quantity into one of kBudgetSlots replicas of the record (the reader sums the replicas)
+    __shared__ double sB[11];
+    if (tid < 11) sB[tid] = 0.0;
+    __syncthreads();
+    const float v[11] = {B.theta, B.src, B.ftu[0], B.ftu[1], B.ftu[2], B.ftu[3],
+                         B.fu[0], B.fu[1], B.fu[2], B.fu[3], B.cells};
+#pragma unroll
+    for (int a = 0; a < 11; ++a) {
+      double d = (double)v[a];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) d += __shfl_xor_sync(0xffffffffu, d, o);
+      if ((tid & 31) == 0 && d != 0.0) atomicAdd(&sB[a], d);
+    }
+    __syncthreads();
+    if (tid < 11 && sB[tid] != 0.0) {
+      const int slot = (bx + 5 * by + 11 * bz) & (kBudgetSlots - 1);
+      atomicAdd(D.budget + slot * kBudgetStride + tid, sB[tid]);
+    }
+  }
+}
+
+}  // namespace ahx

@@ -1,0 +1,143 @@
+// D3Q19 / D3Q7 lattice tables, compile-time q loops and the population storage codecs of the B200 live solver.
+//
+// Lattice tables follow js/live/kernel.js:19-28 of the reference (velocity order, weights 1/3, 1/18, 1/36 and
+// 1/4, 1/8, opposite and z-mirror maps); literals are rounded the way kernel.js:31-33 (fmt) rounds them: the f64
+// fraction rounded once to the arithmetic type.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <stdint.h>
+
+#include <type_traits>
+#include <utility>
+
+namespace ahx {
+
+constexpr int kC19[19][3] = {{0, 0, 0}, {1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1},
+                             {1, 1, 0}, {-1, -1, 0}, {1, -1, 0}, {-1, 1, 0}, {1, 0, 1}, {-1, 0, -1}, {1, 0, -1},
+                             {-1, 0, 1}, {0, 1, 1}, {0, -1, -1}, {0, 1, -1}, {0, -1, 1}};
+constexpr int kC7[7][3] = {{0, 0, 0}, {1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
+
+__host__ __device__ constexpr int find19(int a, int b, int c) {
+  for (int q = 0; q < 19; ++q)
+    if (kC19[q][0] == a && kC19[q][1] == b && kC19[q][2] == c) return q;
+  return -1;
+}
+__host__ __device__ constexpr int find7(int a, int b, int c) {
+  for (int q = 0; q < 7; ++q)
+    if (kC7[q][0] == a && kC7[q][1] == b && kC7[q][2] == c) return q;
+  return -1;
+}
+__host__ __device__ constexpr int opp19(int q) { return find19(-kC19[q][0], -kC19[q][1], -kC19[q][2]); }
+__host__ __device__ constexpr int mirz19(int q) { return find19(kC19[q][0], kC19[q][1], -kC19[q][2]); }
+__host__ __device__ constexpr int opp7(int q) { return find7(-kC7[q][0], -kC7[q][1], -kC7[q][2]); }
+__host__ __device__ constexpr double w19(int q) { return q == 0 ? 1.0 / 3 : (q < 7 ? 1.0 / 18 : 1.0 / 36); }
+__host__ __device__ constexpr double w7(int q) { return q == 0 ? 1.0 / 4 : 1.0 / 8; }
+
+// compile-time loop: f(std::integral_constant<int, 0>) ... f(std::integral_constant<int, N-1>)
+template <int... Qs, class F>
+__host__ __device__ __forceinline__ void static_for_impl(std::integer_sequence<int, Qs...>, F&& f) {
+  (f(std::integral_constant<int, Qs>{}), ...);
+}
+template <int N, class F>
+__host__ __device__ __forceinline__ void static_for(F&& f) {
+  static_for_impl(std::make_integer_sequence<int, N>{}, f);
+}
+
+// Population storage codecs. The state lives in HBM in one of four formats; collision and forcing always run in the
+// arithmetic type Real (f32, or f64 for the FP64 build). 16-bit formats store (f_q - w_q) * scale: the rest
+// equilibrium w_q is subtracted so the stored magnitude is the small deviation, which keeps FP16/BF16 relative
+// rounding on the deviation instead of on O(w) values. Temperature populations g have rest state 0 and are stored
+// scaled only.
+constexpr float kScaleF16 = 16.0f;      // |f - w| < ~0.2 in the UI range: stays well inside FP16 normal range
+constexpr float kScaleG16 = 16.0f;      // theta populations up to ~10 K x w: < 4096 after scaling
+constexpr float kScaleBF16 = 1.0f;      // BF16 has the f32 exponent range: no scaling needed
+
+template <class S>
+struct Codec;
+
+template <>
+struct Codec<float> {
+  using Real = float;
+  static constexpr int kBytes = 4;
+  __device__ __forceinline__ static float load(const float* p) { return __ldg(p); }
+  __device__ __forceinline__ static float dec_f(float v, float /*w*/) { return v; }
+  __device__ __forceinline__ static float dec_g(float v) { return v; }
+  __device__ __forceinline__ static float enc_f(float v, float /*w*/) { return v; }
+  __device__ __forceinline__ static float enc_g(float v) { return v; }
+};
+
+template <>
+struct Codec<double> {
+  using Real = double;
+  static constexpr int kBytes = 8;
+  __device__ __forceinline__ static double load(const double* p) { return __ldg(p); }
+  __device__ __forceinline__ static double dec_f(double v, double /*w*/) { return v; }
+  __device__ __forceinline__ static double dec_g(double v) { return v; }
+  __device__ __forceinline__ static double enc_f(double v, double /*w*/) { return v; }
+  __device__ __forceinline__ static double enc_g(double v) { return v; }
+};
+
+template <>
+struct Codec<__half> {
+  using Real = float;
+  static constexpr int kBytes = 2;
+  __device__ __forceinline__ static __half load(const __half* p) { return __ldg(p); }
+  __device__ __forceinline__ static float dec_f(__half v, float w) {
+    return __fadd_rn(w, __fmul_rn(__half2float(v), 1.0f / kScaleF16));
+  }
+  __device__ __forceinline__ static float dec_g(__half v) { return __fmul_rn(__half2float(v), 1.0f / kScaleG16); }
+  __device__ __forceinline__ static __half enc_f(float v, float w) {
+    return __float2half_rn(__fmul_rn(__fsub_rn(v, w), kScaleF16));
+  }
+  __device__ __forceinline__ static __half enc_g(float v) { return __float2half_rn(__fmul_rn(v, kScaleG16)); }
+};
+
+template <>
+struct Codec<__nv_bfloat16> {
+  using Real = float;
+  static constexpr int kBytes = 2;
+  __device__ __forceinline__ static __nv_bfloat16 load(const __nv_bfloat16* p) { return __ldg(p); }
+  __device__ __forceinline__ static float dec_f(__nv_bfloat16 v, float w) {
+    return __fadd_rn(w, __fmul_rn(__bfloat162float(v), 1.0f / kScaleBF16));
+  }
+  __device__ __forceinline__ static float dec_g(__nv_bfloat16 v) {
+    return __fmul_rn(__bfloat162float(v), 1.0f / kScaleBF16);
+  }
+  __device__ __forceinline__ static __nv_bfloat16 enc_f(float v, float w) {
+    return __float2bfloat16_rn(__fmul_rn(__fsub_rn(v, w), kScaleBF16));
+  }
+  __device__ __forceinline__ static __nv_bfloat16 enc_g(float v) {
+    return __float2bfloat16_rn(__fmul_rn(v, kScaleBF16));
+  }
+};
+
+// Parameter block (kernel.js:44-50): 16 four-byte scalars, then nz x float4 (uin, vin, kbg, 0)
+struct ParamsHead {
+  float tau0, cs2smag, gbeta, prt, kfloor, momfac, srcscale, sigmax;
+  int32_t inflow_w, inflow_e, inflow_s, inflow_n, nsp, nsw, oclip, pad1;
+};
+static_assert(sizeof(ParamsHead) == 64, "parameter head is 64 bytes");
+
+constexpr int kBudgetSlots = 32;    // the budget record is replicated to spread FP64 atomics over 32 addresses
+constexpr int kBudgetStride = 16;   // doubles per slot (11 used)
+
+// One domain's device view. Populations are stored [q][k][j][i] with an x pitch `px` (elements) so every x row
+// starts on a 128-byte boundary: element (q, k, j, i) is at q*qs + (k*ny + j)*px + i.
+struct DomainView {
+  const unsigned char* params;  // ParamsHead + nz float4 profile
+  const uint4* colv;            // NXY records (kt, ktop, cd bits, q bits), row j = 0 south, no pitch
+  const uint32_t* ktop;         // NXY
+  const void* fA;               // current state
+  void* fB;                     // next state
+  const void* gA;
+  void* gB;
+  float4* dbg;                  // (theta, ux, uy, uz) per cell (pitched), or null
+  double* budget;               // per-step FP64 budget accumulators, or null
+  int nx, ny, nz, px;
+  uint32_t ps;                  // plane stride px*ny
+  uint32_t qs;                  // q stride px*ny*nz
+};
+
+}  // namespace ahx

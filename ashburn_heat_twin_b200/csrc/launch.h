@@ -1,0 +1,54 @@
+// Internal launcher interface between the C ABI (api.cu) and the kernel translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "lattice.cuh"
+
+namespace ahx {
+
+struct StepLaunch {
+  int precision;   // ahx_precision
+  int mode;        // 0 none, 1 out, 2 acc
+  bool budget;
+  int block_y;     // threads per block in y (x is one warp)
+  int zslab;       // levels per block
+};
+
+// fused step, IEEE-exact arithmetic (step_exact.cu, built with -fmad=false)
+namespace exact {
+cudaError_t launch_step(const DomainView& D, const StepLaunch& L, cudaStream_t s);
+}
+// fused step, contracted arithmetic (step_fast.cu, built with -fmad=true)
+namespace fast {
+cudaError_t launch_step(const DomainView& D, const StepLaunch& L, cudaStream_t s);
+}
+
+// aux.cu
+cudaError_t launch_init(const DomainView& D, int precision, void* f0, void* f1, cudaStream_t s);
+cudaError_t launch_reinit(const DomainView& D, int precision, const uint32_t* oldk, void* f, void* g,
+                          cudaStream_t s);
+cudaError_t launch_surf(const DomainView& D, int precision, float conv, float* sout, cudaStream_t s);
+cudaError_t launch_vol(const DomainView& D, int precision, int nzv, float volscale, uint32_t* vout,
+                       unsigned* tmax_bits, cudaStream_t s);
+
+struct StatsScratch {
+  double sum[4];          // theta, ke, rho - 1, count
+  unsigned tmax_bits;     // max(theta, 0) as f32 bits
+  unsigned umax_bits;     // max |j|/rho as f32 bits
+  unsigned non_finite;
+  unsigned pad;
+};
+cudaError_t launch_stats(const DomainView& D, int precision, StatsScratch* out, cudaStream_t s);
+
+// layout conversion of one population plane q between the reference layout (f32 or f64, [cell]) and the internal
+// pitched storage; is_g selects the theta codec
+cudaError_t launch_import_plane(const DomainView& D, int precision, const void* ref_plane, int ref_is_f64, void* dst,
+                                int q, int is_g, cudaStream_t s);
+cudaError_t launch_export_plane(const DomainView& D, int precision, const void* src, void* ref_plane, int ref_is_f64,
+                                int q, int is_g, cudaStream_t s);
+
+int element_bytes(int precision);
+
+}  // namespace ahx

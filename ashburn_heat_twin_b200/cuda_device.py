@@ -1,0 +1,316 @@
+"""ctypes binding of libahx.so (include/ahx.h) and the CUDA device object the live solver host drives.
+
+There is no fallback: if the library is missing, fails to load, or no CUDA device is present, constructing a
+CudaDevice raises. The library is built in-tree by ashburn_heat_twin_b200._build (nvcc, sm_100a).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, 'libahx.so')
+
+PRECISIONS = {'fp32': 0, 'fp16': 1, 'bf16': 2, 'fp64': 3}
+ARITH = {'exact': 0, 'fast': 1}
+STATUS = {0: 'AHX_OK', 1: 'AHX_EINVAL', 2: 'AHX_ENOMEM', 3: 'AHX_EDESTROYED', 4: 'AHX_EDEVICE', 5: 'AHX_ETIMEOUT',
+          6: 'AHX_ENONFINITE', 7: 'AHX_EBUSY'}
+MAX_READS = 8
+
+# every symbol include/ahx.h declares
+SYMBOLS = ('ahx_create', 'ahx_destroy', 'ahx_last_error', 'ahx_get_info', 'ahx_set_params', 'ahx_set_columns',
+           'ahx_set_ktop', 'ahx_init_flow', 'ahx_clear_heat', 'ahx_set_parity', 'ahx_step', 'ahx_sync', 'ahx_fence',
+           'ahx_fence_query', 'ahx_read_submit', 'ahx_read_wait', 'ahx_read_state', 'ahx_write_state',
+           'ahx_read_state_f64', 'ahx_write_state_f64', 'ahx_read_dbg', 'ahx_clear_dbg', 'ahx_stats',
+           'ahx_budget_enable', 'ahx_budget_read', 'ahx_set_launch', 'ahx_autotune', 'ahx_time_steps')
+
+
+class AhxError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(msg)
+        self.status = status
+
+
+class Dims(ctypes.Structure):
+    _fields_ = [('nx', ctypes.c_int32), ('ny', ctypes.c_int32), ('nz', ctypes.c_int32),
+                ('precision', ctypes.c_int32), ('device_ordinal', ctypes.c_int32), ('arith', ctypes.c_int32)]
+
+
+class InfoOut(ctypes.Structure):
+    _fields_ = [('nx', ctypes.c_int32), ('ny', ctypes.c_int32), ('nz', ctypes.c_int32), ('px', ctypes.c_int32),
+                ('precision', ctypes.c_int32), ('arith', ctypes.c_int32), ('parity', ctypes.c_int32),
+                ('device_ordinal', ctypes.c_int32), ('steps', ctypes.c_int64), ('state_bytes', ctypes.c_uint64),
+                ('bytes_per_cell', ctypes.c_uint64), ('device_name', ctypes.c_char * 64)]
+
+
+class StatsOut(ctypes.Structure):
+    _fields_ = [('sum_theta', ctypes.c_double), ('sum_ke', ctypes.c_double), ('sum_rho_dev', ctypes.c_double),
+                ('count', ctypes.c_double), ('theta_max', ctypes.c_float), ('umax', ctypes.c_float),
+                ('non_finite', ctypes.c_uint32), ('pad', ctypes.c_uint32)]
+
+
+class BudgetOut(ctypes.Structure):
+    _fields_ = [('theta_sum', ctypes.c_double), ('src_sum', ctypes.c_double),
+                ('face_theta_u', ctypes.c_double * 4), ('face_u', ctypes.c_double * 4), ('cells', ctypes.c_double),
+                ('pad', ctypes.c_double * 5)]
+
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH):
+    """Load libahx.so and declare its signatures. Raises if the library is absent."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise AhxError(-1, f'libahx.so not found at {path}: build it with ashburn_heat_twin_b200._build.build()')
+    L = ctypes.CDLL(path)
+    vp, i, u64p = ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_uint64)
+    H = ctypes.c_void_p
+    sig = {
+        'ahx_create': [ctypes.POINTER(Dims), ctypes.POINTER(H)],
+        'ahx_destroy': [H],
+        'ahx_get_info': [H, ctypes.POINTER(InfoOut)],
+        'ahx_set_params': [H, vp, ctypes.c_size_t],
+        'ahx_set_columns': [H, vp],
+        'ahx_set_ktop': [H, vp, vp],
+        'ahx_init_flow': [H],
+        'ahx_clear_heat': [H],
+        'ahx_set_parity': [H, i],
+        'ahx_step': [H, i, i],
+        'ahx_sync': [H, i],
+        'ahx_time_steps': [H, i, i, i, ctypes.POINTER(ctypes.c_float)],
+        'ahx_fence': [H, u64p],
+        'ahx_fence_query': [H, ctypes.c_uint64, ctypes.POINTER(ctypes.c_int)],
+        'ahx_read_submit': [H, ctypes.c_float, ctypes.c_float, i, i, i, u64p],
+        'ahx_read_wait': [H, ctypes.c_uint64, i, vp, vp, vp, vp, vp],
+        'ahx_read_state': [H, vp, vp],
+        'ahx_write_state': [H, vp, vp],
+        'ahx_read_state_f64': [H, vp, vp],
+        'ahx_write_state_f64': [H, vp, vp],
+        'ahx_read_dbg': [H, vp],
+        'ahx_clear_dbg': [H],
+        'ahx_stats': [H, ctypes.POINTER(StatsOut)],
+        'ahx_budget_enable': [H, i],
+        'ahx_budget_read': [H, ctypes.POINTER(BudgetOut), i],
+        'ahx_set_launch': [H, i, i],
+        'ahx_autotune': [H, i, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                         ctypes.POINTER(ctypes.c_float)],
+    }
+    for name, args in sig.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = ctypes.c_int
+    L.ahx_last_error.argtypes = []
+    L.ahx_last_error.restype = ctypes.c_char_p
+    _lib = L
+    return L
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+class Handle:
+    """Thin owner of one ahx_handle: raises AhxError on any nonzero status."""
+
+    def __init__(self, nx, ny, nz, precision='fp32', device=None, arith='exact'):
+        self.L = load_library()
+        d = Dims(nx=nx, ny=ny, nz=nz, precision=PRECISIONS[precision], arith=ARITH[arith],
+                 device_ordinal=-1 if device is None else int(device))
+        h = ctypes.c_void_p()
+        self._call('ahx_create', ctypes.byref(d), ctypes.byref(h))
+        self.h = h
+        self.nx, self.ny, self.nz = nx, ny, nz
+        self.precision = precision
+
+    def _call(self, name, *args):
+        st = getattr(self.L, name)(*args)
+        if st != 0:
+            msg = self.L.ahx_last_error().decode(errors='replace')
+            raise AhxError(st, msg or f'{name}: {STATUS.get(st, st)}')
+        return st
+
+    def call(self, name, *args):
+        return self._call(name, self.h, *args)
+
+    def info(self):
+        o = InfoOut()
+        self.call('ahx_get_info', ctypes.byref(o))
+        return {k: (getattr(o, k).decode() if k == 'device_name' else getattr(o, k)) for k, _ in InfoOut._fields_}
+
+
+class CudaDevice:
+    """The live solver's device protocol (set_params, set_columns, set_ktop, init_flow, clear_heat, set_parity,
+    step, fence, sync, read, read_state, write_state, read_dbg, clear_dbg, stats, lost, destroy) over libahx.so."""
+
+    def __init__(self, nx, ny, nz, device=None, precision='fp32', arith='exact'):
+        from .solver import Pending   # noqa: F401  (import check)
+        self.hd = Handle(nx, ny, nz, precision=precision, device=device, arith=arith)
+        self.nx, self.ny, self.nz = nx, ny, nz
+        self.N = nx * ny * nz
+        self.precision = precision
+        info = self.hd.info()
+        self.adapter = info['device_name']
+        self._p = 0
+        self._lost = None
+
+    def _c(self, name, *args):
+        try:
+            return self.hd.call(name, *args)
+        except AhxError as e:
+            if e.status == 4:
+                self._lost = str(e)
+            raise
+
+    # host images
+    def set_params(self, b):
+        buf = np.frombuffer(bytes(b), np.uint8)
+        self._c('ahx_set_params', _ptr(buf), buf.nbytes)
+
+    def set_columns(self, colv):
+        a = np.ascontiguousarray(colv, np.uint32)
+        self._c('ahx_set_columns', _ptr(a))
+
+    def set_ktop(self, ktop, oldk):
+        a = np.ascontiguousarray(ktop, np.uint32)
+        o = None if oldk is None else np.ascontiguousarray(oldk, np.uint32)
+        self._c('ahx_set_ktop', _ptr(a), _ptr(o))
+
+    # state
+    def init_flow(self):
+        self._c('ahx_init_flow')
+
+    def clear_heat(self):
+        self._c('ahx_clear_heat')
+
+    def set_parity(self, p):
+        self._c('ahx_set_parity', int(p))
+        self._p = int(p)
+
+    def parity(self):
+        return self._p
+
+    def step(self, n, mode):
+        self._c('ahx_step', int(n), int(mode))
+        self._p ^= (int(n) & 1)
+
+    def fence(self):
+        from .solver import Pending
+        t = ctypes.c_uint64()
+        self._c('ahx_fence', ctypes.byref(t))
+        ticket = t.value
+        done = ctypes.c_int()
+
+        def poll():
+            self._c('ahx_fence_query', ctypes.c_uint64(ticket), ctypes.byref(done))
+            return bool(done.value)
+
+        def wait(timeout_s):
+            import time
+            t0 = time.perf_counter()
+            while not poll():
+                if timeout_s is not None and time.perf_counter() - t0 > timeout_s:
+                    raise AhxError(5, 'live solver: timed out waiting for the GPU')
+                time.sleep(0.0002)
+            return None
+        return Pending(poll=poll, wait=wait)
+
+    def time_steps(self, n, mode=0, timeout_s=None):
+        """queue n steps between two CUDA events on the handle's stream; returns their device time in ms"""
+        ms = ctypes.c_float()
+        self._c('ahx_time_steps', int(n), int(mode), -1 if timeout_s is None else int(timeout_s * 1000),
+                ctypes.byref(ms))
+        self._p ^= (int(n) & 1)
+        return ms.value
+
+    def sync(self, timeout_s=None):
+        self._c('ahx_sync', -1 if timeout_s is None else int(timeout_s * 1000))
+
+    def lost(self):
+        return self._lost
+
+    def read(self, conv, volscale, nzv, want_vol, want_wind, finish):
+        from .solver import Pending
+        t = ctypes.c_uint64()
+        self._c('ahx_read_submit', ctypes.c_float(conv), ctypes.c_float(volscale), int(nzv), int(want_vol),
+                int(want_wind), ctypes.byref(t))
+        ticket = t.value
+        NXY = self.nx * self.ny
+
+        def wait(timeout_s):
+            surf = np.empty(NXY, np.float32)
+            u = np.empty(NXY, np.float32) if want_wind else None
+            v = np.empty(NXY, np.float32) if want_wind else None
+            vb = np.empty(nzv * NXY, np.uint8) if want_vol else None
+            tm = np.zeros(1, np.float32)
+            self._c('ahx_read_wait', ctypes.c_uint64(ticket), -1 if timeout_s is None else int(timeout_s * 1000),
+                    _ptr(surf), _ptr(u), _ptr(v), _ptr(vb), _ptr(tm))
+            return finish((surf, u, v, vb, float(tm[0])))
+        return Pending(poll=lambda: False, wait=wait)
+
+    def read_state(self):
+        f = np.empty(19 * self.N, np.float32)
+        g = np.empty(7 * self.N, np.float32)
+        self._c('ahx_read_state', _ptr(f), _ptr(g))
+        return f, g
+
+    def write_state(self, f, g):
+        fa = None if f is None else np.ascontiguousarray(f, np.float32).ravel()
+        ga = None if g is None else np.ascontiguousarray(g, np.float32).ravel()
+        self._c('ahx_write_state', _ptr(fa), _ptr(ga))
+
+    def read_state_f64(self):
+        f = np.empty(19 * self.N, np.float64)
+        g = np.empty(7 * self.N, np.float64)
+        self._c('ahx_read_state_f64', _ptr(f), _ptr(g))
+        return f, g
+
+    def write_state_f64(self, f, g):
+        fa = None if f is None else np.ascontiguousarray(f, np.float64).ravel()
+        ga = None if g is None else np.ascontiguousarray(g, np.float64).ravel()
+        self._c('ahx_write_state_f64', _ptr(fa), _ptr(ga))
+
+    def read_dbg(self):
+        d = np.empty(4 * self.N, np.float32)
+        self._c('ahx_read_dbg', _ptr(d))
+        return d
+
+    def clear_dbg(self):
+        self._c('ahx_clear_dbg')
+
+    def stats(self):
+        o = StatsOut()
+        self._c('ahx_stats', ctypes.byref(o))
+        return dict(sumTheta=o.sum_theta, sumKE=o.sum_ke, sumRhoDev=o.sum_rho_dev, count=int(o.count),
+                    thetaMax=float(o.theta_max), nonFinite=int(o.non_finite), umax=float(o.umax))
+
+    def budget_enable(self, on=True):
+        self._c('ahx_budget_enable', int(bool(on)))
+
+    def budget_read(self, reset=False):
+        o = BudgetOut()
+        self._c('ahx_budget_read', ctypes.byref(o), int(bool(reset)))
+        return dict(theta_sum=o.theta_sum, src_sum=o.src_sum, face_theta_u=list(o.face_theta_u),
+                    face_u=list(o.face_u), cells=o.cells)
+
+    def set_launch(self, block_y=0, zslab=0):
+        self._c('ahx_set_launch', int(block_y), int(zslab))
+
+    def autotune(self, steps_per_trial=4):
+        by, zs, ms = ctypes.c_int(), ctypes.c_int(), ctypes.c_float()
+        self._c('ahx_autotune', int(steps_per_trial), ctypes.byref(by), ctypes.byref(zs), ctypes.byref(ms))
+        return by.value, zs.value, ms.value
+
+    def info(self):
+        return self.hd.info()
+
+    def destroy(self):
+        if self.hd is not None:
+            try:
+                self.hd.call('ahx_destroy')
+            finally:
+                self.hd = None

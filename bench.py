@@ -1,0 +1,292 @@
+#!/usr/bin/env python3
+"""Benchmark of the fused D3Q19 + D3Q7 live-solver step on one B200 per rank.
+
+Workload: the 600 x 600 x 64 domain at 10 m (23.04 M cells), seeded synthetic terrain and buildings (24 hills with
+0-40 m relief, 4,000 buildings, 211 data-center roofs at 400 W/m^2), inflow 3.5 m/s from 200 deg with power-law
+exponent 0.2, FP32 populations, pull scheme. Metric: GLUPS = all nx*ny*nz cells updated per second (the reference's
+MLUPS convention, js/live/solver.js:482), whole job over all ranks.
+
+`value` is device time (CUDA events on the solver's own stream) with the state resident in HBM; the state (4.8 GB)
+is far larger than L2, so no flush is needed between steps. `e2e` runs the same stepping through the public API
+(create_live_solver / setMet / step / read) with host buffers: every frame uploads a parameter block from host
+memory, advances F steps and reads back the near-surface fields and the u8 volume, as the live app does.
+
+--gpus N runs N independent replicas, one per rank (the path does not shard: "replicas only", weak scaling).
+--impl reference times the CPU restatement of the reference kernels (the reference itself is WebGPU/WGSL and cannot
+run here) on all host cores, rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = '600x600x64 cells at 10 m (23.04 M), synthetic seed 2: 24 hills 0-40 m, 4000 buildings, 211 DC roofs'
+METRIC = 'GLUPS (all cells) of the fused D3Q19+D3Q7 step, 600x600x64'
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def make_solver(backend=None, device=None, precision='fp32', arith='exact'):
+    from ashburn_heat_twin_b200 import solver as S
+    from ashburn_heat_twin_b200 import synth
+    st = synth.make_static10(synth.C2)
+    kw = dict(static=st, dx=10, allowAnyDx=True, heightM=640, u10Max=8, alpha=0.2, met=synth.C2_MET,
+              existingFlux=400)
+    if backend is None:
+        from ashburn_heat_twin_b200.cuda_device import CudaDevice
+
+        def backend(nx, ny, nz):
+            return CudaDevice(nx, ny, nz, device=device, precision=precision, arith=arith)
+    return S.create_live_solver(backend=backend, **kw)
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, 'MEASURED_PEAKS.json')
+    try:
+        d = json.load(open(p))
+        return float(d['hbm_gbs']), 'measured'
+    except Exception:
+        return 6650.0, 'fallback'
+
+
+def profile_traffic(precision):
+    """DRAM bytes per launch of the step kernel from the committed ncu summary, scaled to the 600x600x64 launch."""
+    p = os.path.join(ROOT, 'profiles', f'step_{precision}_traffic.json')
+    try:
+        return json.load(open(p))['dram_bytes_per_launch_scaled']
+    except Exception:
+        return None
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clock and throttle reasons during the timed region."""
+    Q = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,'
+         'clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,'
+         'clocks_event_reasons.sw_power_cap')
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.f = tempfile.NamedTemporaryFile('w+', suffix='.csv', delete=False)
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(['nvidia-smi', f'--query-gpu={self.Q}', '--format=csv,noheader,nounits',
+                                       '-lms', '100', '-i', str(self.gpu)], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        time.sleep(0.2)
+        if self.p is not None:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except Exception:
+                self.p.kill()
+
+    def summary(self):
+        try:
+            rows = [r.split(',') for r in open(self.f.name).read().strip().splitlines() if r.strip()]
+        except Exception:
+            rows = []
+        os.unlink(self.f.name)
+        if not rows:
+            return dict(sm_mhz=None, sm_max_mhz=None, reasons=['unsampled'])
+        sm = [float(r[1]) for r in rows]
+        mx = max(float(r[2]) for r in rows)
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
+        reasons = sorted({names[i] for r in rows for i, v in enumerate(r[5:9]) if v.strip() == 'Active'})
+        return dict(sm_mhz=statistics.median(sm), sm_max_mhz=mx, reasons=reasons, samples=len(rows),
+                    power_w_max=max(float(r[3]) for r in rows if r[3].strip().replace('.', '', 1).isdigit())
+                    if any(r[3].strip().replace('.', '', 1).isdigit() for r in rows) else None)
+
+
+def cpu_baseline(seconds=10.0, max_steps=30):
+    """The oracle (CPU restatement of the reference kernels) on full 600x600x64 steps, all host threads."""
+    import numpy as np
+    from oracle import oracle as O
+    s = make_solver(backend=lambda nx, ny, nz: O.OracleDevice(nx, ny, nz))
+    threads = O.max_threads()
+    dev = s._dev
+    t0 = time.perf_counter()
+    dev.step(1, 0)
+    t1 = time.perf_counter() - t0
+    n = int(max(1, min(max_steps, np.ceil(seconds / max(t1, 1e-3)))))
+    t0 = time.perf_counter()
+    dev.step(n, 0)
+    t = time.perf_counter() - t0
+    cells = s.info['nCells']
+    s.destroy()
+    return dict(value=cells * n / t / 1e9, unit='GLUPS', cores=threads, kind='port',
+                sample=f'{n} full steps of the 600x600x64 domain ({cells * n / 1e6:.0f} M cell updates, {t:.1f} s)')
+
+
+def run_reference(a, rank):
+    if rank != 0:
+        return 0
+    import numpy as np
+    from oracle import oracle as O
+    s = make_solver(backend=lambda nx, ny, nz: O.OracleDevice(nx, ny, nz))
+    dev = s._dev
+    dev.step(a.warmup, 0)
+    t0 = time.perf_counter()
+    dev.step(a.steps, 0)
+    t = time.perf_counter() - t0
+    cells = s.info['nCells']
+    v = cells * a.steps / t / 1e9
+    out = dict(metric=METRIC, value=v, unit='GLUPS', n_gpus=a.gpus, steps=a.steps, warmup=a.warmup,
+               ms_per_step=t / a.steps * 1e3, higher_is_better=True, scaling='weak', vs_baseline=None, dtype='f32',
+               data='synthetic', impl='reference',
+               config=dict(workload=WORKLOAD, precision='fp32', scheme='pull', parallelism='replicas'),
+               cpu_baseline=dict(value=v, unit='GLUPS', cores=O.max_threads(), kind='port',
+                                 sample=f'{a.steps} full steps after {a.warmup} warm-up steps'),
+               e2e=dict(value=v, unit='GLUPS', h2d_bytes_per_step=0, d2h_bytes_per_step=0))
+    s.destroy()
+    del np
+    print(json.dumps(out), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=20)
+    ap.add_argument('--warmup', type=int, default=5)
+    ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
+    ap.add_argument('--precision', default='fp32', choices=['fp32', 'fp16', 'bf16', 'fp64'])
+    ap.add_argument('--arith', default='exact', choices=['exact', 'fast'])
+    ap.add_argument('--frame', type=int, default=10, help='steps per e2e frame (setMet + step(F) + read())')
+    ap.add_argument('--no-cpu-baseline', action='store_true')
+    ap.add_argument('--no-autotune', action='store_true')
+    a = ap.parse_args()
+    a.warmup = max(a.warmup, 3)
+
+    rank = int(os.environ.get('RANK', '0'))
+    world = int(os.environ.get('WORLD_SIZE', '1'))
+    local = int(os.environ.get('LOCAL_RANK', '0'))
+    if a.impl == 'reference':
+        return run_reference(a, rank)
+
+    import torch
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device('cuda', local))
+    from ashburn_heat_twin_b200 import _build
+    _build.build()
+    s = make_solver(device=local, precision=a.precision, arith=a.arith)
+    dev = s._dev
+    nx, ny, nz = s.info['nx'], s.info['ny'], s.info['nz']
+    cells = nx * ny * nz
+    fluid = s.info['nFluid']
+    tune = None
+    if not a.no_autotune:
+        tune = dev.autotune(3)
+        log(f'[rank {rank}] autotune: block_y {tune[0]} zslab {tune[1]} {tune[2]:.3f} ms/step')
+    dev.time_steps(a.warmup)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize(local)
+
+    barrier()
+    with Clocks(local) as clk:
+        barrier()
+        ms = dev.time_steps(a.steps)
+        barrier()
+    clocks = clk.summary()
+    ms_all = ms
+    if dist is not None:
+        t = torch.tensor([ms], device=f'cuda:{local}', dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_all = float(t.item())
+    value = world * cells * a.steps / (ms_all / 1e3) / 1e9
+
+    # roofline of the step kernel (one launch per step): algorithmic bytes = fluid cells x (read + write of 19 f and
+    # 7 g populations) at the storage width
+    esize = {'fp32': 4, 'fp16': 2, 'bf16': 2, 'fp64': 8}[a.precision]
+    bytes_launch = fluid * 52 * esize
+    launch_ms = ms / a.steps
+    achieved = bytes_launch / (launch_ms / 1e3) / 1e9
+    peak, peak_kind = measured_peaks()
+    roof = dict(bound='hbm', achieved=achieved, peak=peak, unit='GB/s', frac=achieved / peak,
+                traffic=profile_traffic(a.precision), peak_source=peak_kind,
+                bytes_per_launch=bytes_launch, launch_ms=launch_ms)
+
+    # end to end through the public API with host buffers
+    from ashburn_heat_twin_b200 import synth
+    F = a.frame
+    frames = max(3, a.steps // 2)
+    met = dict(synth.C2_MET)
+    pend = []
+    s.setMet(met)
+    s.step(F)
+    s.read().result()
+    barrier()
+    t0 = time.perf_counter()
+    for fr in range(frames):
+        met['u10'] = 3.5 + 0.01 * (fr % 5)          # a new parameter block every frame (host -> device)
+        s.setMet(met)
+        s.step(F)
+        pend.append(s.read(vol=True, wind=True))
+        if len(pend) > 2:
+            pend.pop(0).result()
+    for p in pend:
+        p.result()
+    barrier()
+    e2e_s = time.perf_counter() - t0
+    if dist is not None:
+        t = torch.tensor([e2e_s], device=f'cuda:{local}', dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    NXY = nx * ny
+    h2d = len(s._params)
+    d2h = 3 * NXY * 4 + s.nzv * NXY + 4
+    e2e = dict(value=world * cells * F * frames / e2e_s / 1e9, unit='GLUPS', h2d_bytes_per_step=h2d / F,
+               d2h_bytes_per_step=d2h / F, frame_steps=F, frames=frames,
+               per_frame='setMet (parameter block H2D) + step(F) + read(vol, wind) D2H')
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        s_steps = s._steps
+        cpu = cpu_baseline()
+        del s_steps
+    out = dict(metric=METRIC, value=value, unit='GLUPS', n_gpus=world, steps=a.steps, warmup=a.warmup,
+               ms_per_step=ms_all / a.steps, higher_is_better=True, scaling='weak', vs_baseline=None,
+               dtype={'fp32': 'f32', 'fp16': 'f16-store/f32', 'bf16': 'bf16-store/f32', 'fp64': 'f64'}[a.precision],
+               data='synthetic (seeded terrain and buildings; no public dataset involved)',
+               config=dict(workload=WORKLOAD, precision=a.precision, arith=a.arith, scheme='pull',
+                           parallelism=f'replicas x{world}', fluid_cells=fluid, l2='state 4.8 GB >> 126 MB L2',
+                           launch=dict(block_y=tune[0], zslab=tune[1]) if tune else None),
+               roofline=roof, cpu_baseline=cpu, e2e=e2e, gpu_launches=a.steps, clocks=clocks,
+               glups_fluid=world * fluid * a.steps / (ms_all / 1e3) / 1e9)
+    s.destroy()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    return 0
+
+
+if __name__ == '__main__':
+    sys.exit(main())

@@ -1,0 +1,190 @@
+/* ahx.h — C ABI of the B200 live solver: the coupled D3Q19 flow + D3Q7 heat lattice-Boltzmann step of the
+ * ashburn-heat-twin live mode, on CUDA (sm_100a).
+ *
+ * The host keeps the domain and parameter math (js/live/domain.js and the parameter code of js/live/solver.js in the
+ * reference) and hands this library the same byte images the reference's WebGPU backend receives:
+ *   - the parameter block, 64 + 16*nz bytes (kernel.js:36-50, written by solver.js:225-242);
+ *   - the per-column records, NXY x vec4<u32> = (kt, ktop, cd f32 bits, q f32 bits) (solver.js:359-376);
+ *   - the ktop plane, NXY x u32 (solver.js:338).
+ * Populations are exchanged in the reference's layout, f32 [q][cell] with cell = (k*ny + j)*nx + i, j = 0 at the
+ * south edge (kernel.js:17), whatever the internal storage format.
+ *
+ * Conventions: every call returns an ahx_status (0 = ok). On failure ahx_last_error() returns a readable message for
+ * the calling thread. A handle owns all device memory it uses; host buffers are always the caller's and are copied
+ * in or out before the call returns (or, for ahx_read_submit, before ahx_read_wait returns). Calls on one handle are
+ * serialised by an internal mutex. Device work is queued on the handle's CUDA stream and returns at once unless the
+ * call says otherwise. A CUDA error on the handle's context makes the handle "lost": later calls return
+ * AHX_EDEVICE (the reference's device-lost state, solver.js:139,219-222). No call aborts or traps.
+ */
+#ifndef AHX_H
+#define AHX_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  AHX_OK = 0,
+  AHX_EINVAL = 1,      /* bad argument or size */
+  AHX_ENOMEM = 2,      /* device or pinned-host allocation failed (solver.js:142-156 out-of-memory scope) */
+  AHX_EDESTROYED = 3,  /* handle already destroyed (solver.js:220 "live solver: destroyed") */
+  AHX_EDEVICE = 4,     /* CUDA error: the handle is lost (solver.js:221) */
+  AHX_ETIMEOUT = 5,    /* a bounded wait expired; the work is still queued */
+  AHX_ENONFINITE = 6,  /* a check found NaN/Inf in the state */
+  AHX_EBUSY = 7        /* no free read slot (more than AHX_MAX_READS reads in flight) */
+} ahx_status;
+
+typedef enum { AHX_FP32 = 0, AHX_FP16 = 1, AHX_BF16 = 2, AHX_FP64 = 3 } ahx_precision;
+
+/* step output modes (kernel.js:427-428; solver.js:551-558 stepOut / stepAcc) */
+typedef enum { AHX_MODE_NONE = 0, AHX_MODE_OUT = 1, AHX_MODE_ACC = 2 } ahx_mode;
+
+/* arithmetic variant of the fused step: EXACT evaluates every expression in the reference's order with IEEE-rounded
+ * f32 operations and no contraction (bit-identical to the CPU restatement); FAST lets the compiler contract into FMA. */
+typedef enum { AHX_ARITH_EXACT = 0, AHX_ARITH_FAST = 1 } ahx_arith;
+
+#define AHX_MAX_READS 8
+
+typedef struct ahx_handle ahx_handle;
+
+typedef struct {
+  int32_t nx, ny, nz;        /* grid (reference: dom.nx, ny, nz) */
+  int32_t precision;         /* ahx_precision of the stored populations */
+  int32_t device_ordinal;    /* CUDA device; -1 = current */
+  int32_t arith;             /* ahx_arith */
+} ahx_dims;
+
+typedef struct {
+  int32_t nx, ny, nz, px;    /* px: internal x pitch in elements */
+  int32_t precision, arith, parity, device_ordinal;
+  int64_t steps;             /* steps run on this handle since creation */
+  uint64_t state_bytes;      /* bytes of both population buffers */
+  uint64_t bytes_per_cell;   /* algorithmic bytes moved per fluid cell update (read + write of f and g) */
+  char device_name[64];
+} ahx_info_out;
+
+/* diagnostics over all fluid cells of the current state (kernel.js:580-633 genStatsWGSL, solver.js:559-575):
+ * per-cell f32 values summed in FP64 */
+typedef struct {
+  double sum_theta;          /* sum of theta (K) */
+  double sum_ke;             /* sum of 0.5|j|^2/rho (lattice units) */
+  double sum_rho_dev;        /* sum of rho - 1 */
+  double count;              /* fluid cells with finite rho and theta */
+  float theta_max;           /* max(theta, 0) */
+  float umax;                /* max |j|/rho (lattice units) */
+  uint32_t non_finite;       /* cells with non-finite rho or theta */
+  uint32_t pad;
+} ahx_stats_out;
+
+/* Per-step FP64 budget record, accumulated inside the fused step when enabled (no counterpart in the reference,
+ * which computes the heat budget offline from time-mean fields, tools/live/validate_live.py:226-240). Lateral-face
+ * sums use the post-stream moments of the face cells: theta*u (K lattice-velocity) and u (lattice velocity). */
+typedef struct {
+  double theta_sum;          /* sum of pre-collision theta over fluid cells */
+  double src_sum;            /* sum of the per-column source S (K/step) injected this step */
+  double face_theta_u[4];    /* sum over face cells of theta*u_n: west (ux), east (ux), south (uy), north (uy) */
+  double face_u[4];          /* sum over face cells of u_n, same faces */
+  double cells;              /* fluid cells updated */
+  double pad[5];
+} ahx_budget_out;
+
+/* --- lifetime ------------------------------------------------------------------------------------------------ */
+
+/* createLiveSolver's device part (solver.js:137-196 _init: buffers; pipelines are compiled ahead of time here).
+ * Allocates both population buffers, column and ktop planes and the read pool. */
+ahx_status ahx_create(const ahx_dims* dims, ahx_handle** out);
+
+/* destroy() (solver.js:485-493): idempotent for a valid handle; releases everything. */
+ahx_status ahx_destroy(ahx_handle* h);
+
+/* thread-local message of the last failure on this thread */
+const char* ahx_last_error(void);
+
+ahx_status ahx_get_info(ahx_handle* h, ahx_info_out* out);
+
+/* --- host images (solver.js:225-242, 323-376) ------------------------------------------------------------------ */
+
+/* the parameter block: bytes == 64 + 16*nz (kernel.js:36) */
+ahx_status ahx_set_params(ahx_handle* h, const void* params, size_t bytes);
+
+/* NXY records of 4 x u32 (kt, ktop, cd bits, q bits) */
+ahx_status ahx_set_columns(ahx_handle* h, const uint32_t* colv);
+
+/* the ktop plane; when old_ktop is not NULL, cells that turned from solid to fluid (k in [ktop, min(old_ktop, nz)))
+ * get rest equilibrium and theta = 0 in the current state (solver.js:336-349 + kernel.js:557-575 genReinitWGSL) */
+ahx_status ahx_set_ktop(ahx_handle* h, const uint32_t* ktop, const uint32_t* old_ktop);
+
+/* --- state (solver.js:288-293, 380-398) ------------------------------------------------------------------------ */
+
+/* f -> equilibrium with the inflow profile at the local height above terrain in both buffers (kernel.js:524-553
+ * genInitWGSL); theta kept */
+ahx_status ahx_init_flow(ahx_handle* h);
+
+/* g -> 0 in both buffers (solver.js:383,394 clearBuffer) */
+ahx_status ahx_clear_heat(ahx_handle* h);
+
+/* set the ping-pong parity (resetFlow sets 0, solver.js:396) */
+ahx_status ahx_set_parity(ahx_handle* h, int parity);
+
+/* --- stepping (solver.js:401-427) ------------------------------------------------------------------------------- */
+
+/* queue n fused steps (kernel.js:395-431). mode AHX_MODE_OUT writes (theta, ux, uy, uz) on the last step,
+ * AHX_MODE_ACC accumulates it on every step. Returns at once. */
+ahx_status ahx_step(ahx_handle* h, int n, int mode);
+
+/* queue n steps bracketed by two CUDA events recorded on the handle's own stream, wait for them (bounded by
+ * timeout_ms, < 0 = no limit) and return the device time between the events in *ms */
+ahx_status ahx_time_steps(ahx_handle* h, int n, int mode, int timeout_ms, float* ms);
+
+/* wait for all queued work; timeout_ms < 0 waits without limit. AHX_ETIMEOUT leaves the work queued. */
+ahx_status ahx_sync(ahx_handle* h, int timeout_ms);
+
+/* a fence after the work queued so far: ahx_fence returns a ticket, ahx_fence_query reports 1 when it passed */
+ahx_status ahx_fence(ahx_handle* h, uint64_t* ticket);
+ahx_status ahx_fence_query(ahx_handle* h, uint64_t ticket, int* done);
+
+/* --- read-back (solver.js:439-471; kernel.js:435-520) ----------------------------------------------------------- */
+
+/* queue the near-surface and volume extraction of the current state behind the queued steps and start the copy to
+ * pinned staging on a second stream; stepping may continue meanwhile. conv = dx/dt (f32), volscale = 255/volMax
+ * (f32), nzv levels of u8 volume. Returns a ticket for ahx_read_wait. */
+ahx_status ahx_read_submit(ahx_handle* h, float conv, float volscale, int nzv, int want_vol, int want_wind,
+                           uint64_t* ticket);
+
+/* wait (bounded) for a submitted read and copy it out: surf/u/v NXY f32 north-up (u, v may be NULL), vol
+ * nzv*NXY u8 (may be NULL), theta_max the unclamped max theta over the fluid cells of those levels. */
+ahx_status ahx_read_wait(ahx_handle* h, uint64_t ticket, int timeout_ms, float* surf, float* u, float* v,
+                         uint8_t* vol, float* theta_max);
+
+/* --- validation hooks (solver.js:496-578 _dbg) ------------------------------------------------------------------ */
+
+ahx_status ahx_read_state(ahx_handle* h, float* f, float* g);          /* 19N + 7N f32, reference layout */
+ahx_status ahx_write_state(ahx_handle* h, const float* f, const float* g); /* either may be NULL */
+ahx_status ahx_read_state_f64(ahx_handle* h, double* f, double* g);    /* FP64 handles only */
+ahx_status ahx_write_state_f64(ahx_handle* h, const double* f, const double* g);
+ahx_status ahx_read_dbg(ahx_handle* h, float* dbg4);                   /* 4N f32 (theta, ux, uy, uz) per cell */
+ahx_status ahx_clear_dbg(ahx_handle* h);
+ahx_status ahx_stats(ahx_handle* h, ahx_stats_out* out);               /* synchronous */
+
+/* --- budgets ---------------------------------------------------------------------------------------------------- */
+
+/* enable (1) / disable (0) the per-step FP64 budget accumulation fused into the step; while enabled each step adds
+ * into a device record, read (and optionally reset) with ahx_budget_read (synchronous). */
+ahx_status ahx_budget_enable(ahx_handle* h, int on);
+ahx_status ahx_budget_read(ahx_handle* h, ahx_budget_out* out, int reset);
+
+/* --- tuning ----------------------------------------------------------------------------------------------------- */
+
+/* launch shape of the fused step: threads per block in y (x is one warp), z-slab depth in levels; 0 = keep */
+ahx_status ahx_set_launch(ahx_handle* h, int block_y, int zslab);
+/* time candidate launch shapes on scratch copies of the state and keep the fastest; the state is not advanced */
+ahx_status ahx_autotune(ahx_handle* h, int steps_per_trial, int* best_block_y, int* best_zslab, float* best_ms);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* AHX_H */

@@ -1,0 +1,213 @@
+"""The CUDA path against the reference's archived results on the real Ashburn domain
+(tests/live/validation_summary.json of the reference, extracted into tests/golden/kat_live.json).
+
+Tolerances: the reference's own WebGPU-vs-numba agreement is 3e-6 relative on read() scalars after 300 steps and
+about 1e-5 after 2300 steps; the 600 s mean near-ground theta agrees to 4.3e-5 rel-L2 after 10,910 steps.
+"""
+import numpy as np
+import pytest
+
+from ashburn_heat_twin_b200 import params as PM
+from tests.helpers import MET_AUG25, campus_list, cuda_backend, real_solver, surf_stats
+
+pytestmark = pytest.mark.gpu
+
+# met of each short run (validate.html makeSolver: query u10/dir override the 25 Aug values, u* then defaults)
+SHORT = {
+    'p30a': dict(dx=30, met=MET_AUG25, flux=400),
+    'p30b': dict(dx=30, met=MET_AUG25, flux=400),
+    'p20': dict(dx=20, met=MET_AUG25, flux=400),
+    'p40': dict(dx=40, met=dict(u10=6, dirFrom=75, wstar=1.67, blh=903), flux=400),
+    'p40w': dict(dx=40, met=dict(u10=1, dirFrom=300, wstar=0, blh=903), flux=800),
+}
+
+
+def _short(kat, tag, precision='fp32', arith='exact'):
+    k = kat[tag]
+    c = SHORT[tag]
+    s = real_solver(cuda_backend(precision, arith), dx=c['dx'], met=c['met'], existingFlux=c['flux'],
+                    nsw=k['params']['nsw'], outflowClip=bool(k['params']['oclip']))
+    s.setNewCampuses(campus_list(k['campus']))
+    if k['pre']:
+        s.step(k['pre']).result()
+    s._dbg.stepOut(k['steps']).result()
+    r = s.read(vol=True, wind=True, volMax=3).result()
+    return s, r
+
+
+@pytest.mark.parametrize('tag,rtol', [('p30a', 3e-6), ('p30b', 2e-5), ('p20', 2e-5), ('p40', 2e-5)])
+def test_short_runs(kat, tag, rtol):
+    k = kat[tag]
+    s, r = _short(kat, tag)
+    ss = surf_stats(r)
+    assert s._dbg.domain()['inflow'] == k['inflow']
+    assert s.info['nFluid'] == k['info']['nFluid']
+    assert r['heatMW'] == pytest.approx(k['heatMW'], rel=1e-12)
+    assert ss['nan'] == 0
+    assert r['thetaMax'] == pytest.approx(k['thetaMax'], rel=rtol)
+    assert ss['surfMax'] == pytest.approx(k['surfMax'], rel=rtol)
+    assert ss['surfMean'] == pytest.approx(k['surfMean'], rel=rtol)
+    assert ss['windMean'] == pytest.approx(k['windMean'], rel=rtol)
+    s.destroy()
+
+
+def test_short_p40w(kat):
+    """1 m/s convective case at 40 m with campuses A+B and 800 W/m^2 (the weakest-wind validation run)."""
+    k = kat['p40w']
+    s, r = _short(kat, 'p40w')
+    ss = surf_stats(r)
+    assert r['heatMW'] == pytest.approx(k['heatMW'], rel=1e-12)
+    assert r['thetaMax'] == pytest.approx(k['thetaMax'], rel=1e-4)
+    assert ss['surfMean'] == pytest.approx(k['surfMean'], rel=1e-4)
+    s.destroy()
+
+
+def test_fast_arithmetic_p30a(kat):
+    k = kat['p30a']
+    s, r = _short(kat, 'p30a', arith='fast')
+    assert r['thetaMax'] == pytest.approx(k['thetaMax'], rel=5e-6)
+    assert surf_stats(r)['surfMean'] == pytest.approx(k['surfMean'], rel=5e-6)
+    s.destroy()
+
+
+def _heat_diag(mean, fluid, dx, q, dt):
+    """tools/live/validate_live.py:226-240 of the reference (product of time-mean fields)."""
+    th, u, v, w = mean
+    face = lambda arr, sl: float((arr[sl] * fluid[sl]).sum() * dx * dx)
+    hw = face(th * u, (slice(None), slice(None), 0)); he = face(th * u, (slice(None), slice(None), -1))
+    hs = face(th * v, (slice(None), 0, slice(None))); hn = face(th * v, (slice(None), -1, slice(None)))
+    out_W = PM.RHO_CP * (he - hw + hn - hs)
+    in_W = float(q.astype(np.float64).sum() * PM.RHO_CP * dx ** 3 / dt)
+    content = float(np.where(fluid, th, 0).sum() * PM.RHO_CP * dx ** 3 / 1e6)
+    qw = face(u, (slice(None), slice(None), 0)); qe = face(u, (slice(None), slice(None), -1))
+    qs = face(v, (slice(None), 0, slice(None))); qn = face(v, (slice(None), -1, slice(None)))
+    thru = abs(qw) + abs(qe) + abs(qs) + abs(qn)
+    return dict(heat_injected_MW=in_W / 1e6, heat_advected_out_MW=out_W / 1e6, heat_content_MJ=content,
+                mass_imbalance_frac=abs(qw - qe + qs - qn) / max(thru, 1e-9))
+
+
+def _plume(th, ktop, dca, dx):
+    """tools/live/validate_live.py:243-255 of the reference, north-up [z, row, col]."""
+    nz, ny, nx = th.shape
+    kk = np.arange(nz)[:, None, None]
+    fluid = kk >= ktop[None]
+    thp = np.where(fluid, np.clip(th, 0, None), 0)
+    yy, xx = np.mgrid[0:ny, 0:nx]
+    X = (xx + 0.5) * dx
+    Y = (ny - yy - 0.5) * dx
+    sx, sy = (dca * X).sum() / dca.sum(), (dca * Y).sum() / dca.sum()
+    tot = thp.sum(axis=0)
+    cx, cy = (tot * X).sum() / tot.sum(), (tot * Y).sum() / tot.sum()
+    zagl = (kk - ktop[None] + 0.5) * dx
+    return dict(displacement_m=float(np.hypot(cx - sx, cy - sy)),
+                bearing_deg=float((np.degrees(np.arctan2(cx - sx, cy - sy)) + 360) % 360),
+                heat_weighted_height_agl_m=float((thp * zagl).sum() / thp.sum()))
+
+
+def test_long_L30c(kat):
+    """25 Aug 2024 at 30 m: 2200 s spin-up then a 600 s mean accumulated every step (validate.html `long`), with the
+    outlet clip and sponge width 5. Surface mean theta, heat budget, mass imbalance and plume against the reference."""
+    k = kat['L30c']
+    s = real_solver(cuda_backend('fp32', 'exact'), dx=30)
+    assert s.info['dt'] == k['dt'] and s._nsw == k['nsw']
+    s.setNewCampuses([])
+    s.step(k['nspin']).result()
+    s._dbg.clearDbg()
+    s._dbg.stepAcc(k['navg']).result()
+    st = s._dbg.stats()
+    fin = k['final']
+    assert st['steps'] == fin['step'] and st['nonFinite'] == 0
+    assert st['thetaMax'] == pytest.approx(fin['thetaMax'], rel=1e-4)
+    assert st['heatContentMJ'] == pytest.approx(fin['heatMJ'], rel=1e-4)
+    assert st['keMean'] == pytest.approx(fin['ke'], rel=1e-4)
+    nx, ny, nz = s.info['nx'], s.info['ny'], s.info['nz']
+    conv = s._conv
+    acc = s._dbg.readDbg().reshape(nz, ny, nx, 4)
+    mw = np.moveaxis(acc, -1, 0).astype(np.float64) / k['navg']
+    mw[1:] *= conv
+    ktop = s._ktopS.reshape(ny, nx).astype(np.int64)
+    fluid = np.arange(nz)[:, None, None] >= ktop[None]
+    jj, ii = np.meshgrid(np.arange(ny), np.arange(nx), indexing='ij')
+    surf = mw[0][ktop, jj, ii][::-1]
+    want = k['surface_mean_theta_webgpu']
+    assert surf.max() == pytest.approx(want['max'], rel=1e-4)
+    assert surf.mean() == pytest.approx(want['mean'], rel=1e-4)
+    hb = _heat_diag(mw, fluid, 30.0, s._q.reshape(ny, nx), s.info['dt'])
+    wb = k['heat_budget_webgpu']
+    assert hb['heat_injected_MW'] == pytest.approx(wb['heat_injected_MW'], rel=1e-9)
+    assert hb['heat_advected_out_MW'] == pytest.approx(wb['heat_advected_out_MW'], rel=1e-4)
+    assert hb['heat_content_MJ'] == pytest.approx(wb['heat_content_MJ'], rel=1e-4)
+    assert hb['mass_imbalance_frac'] == pytest.approx(wb['mass_imbalance_frac'], rel=2e-2)
+    dca = s._q.reshape(ny, nx)[::-1].astype(np.float64)
+    pl = _plume(mw[0][:, ::-1], ktop[::-1], dca, 30.0)
+    wp = k['plume_webgpu']
+    assert pl['displacement_m'] == pytest.approx(wp['displacement_m'], rel=1e-4)
+    assert pl['bearing_deg'] == pytest.approx(wp['bearing_deg'], abs=0.01)
+    assert pl['heat_weighted_height_agl_m'] == pytest.approx(wp['heat_weighted_height_agl_m'], rel=1e-4)
+    s.destroy()
+
+
+def test_api20(kat):
+    """The reference's interface test at 20 m (validate.html `api`, tag api20) through the CUDA backend."""
+    from ashburn_heat_twin_b200 import solver as S
+    k = kat['api20']
+    with pytest.raises(S.LiveSolverError) as e:
+        real_solver(cuda_backend(), dx=25)
+    assert 'rejected: ' + str(e.value) == k['badDx']
+    with pytest.raises(S.LiveSolverError) as e:
+        real_solver(cuda_backend(), u10Max=0)
+    assert 'rejected: ' + str(e.value) == k['badU10Max']
+    s = real_solver(cuda_backend(), dx=20)
+    assert s.info['nFluid'] == k['info']['nFluid']
+    s.step(300).result()
+    r0 = s.read(vol=False, wind=False).result()
+    assert r0['thetaMax'] == pytest.approx(k['readNoVolNoWind']['thetaMax'], rel=3e-6)
+    # 8 concurrent reads while stepping: each sees the state (and simTime) at its submission
+    ps = []
+    for _ in range(8):
+        ps.append(s.read())
+        s.step(5)
+    rs = [p.result() for p in ps]
+    assert [round(r['simTime'], 2) for r in rs] == k['concurrentReads']
+    s.setNewCampuses(campus_list('AB'))
+    nf1, rA = s.info['nFluid'], s.read().result()
+    s.step(1000).result()
+    stA = s._dbg.stats()
+    s.setNewCampuses([])
+    nf2 = s.info['nFluid']
+    s.step(1000).result()
+    stB, rB = s._dbg.stats(), s.read().result()
+    kc = k['campuses']
+    assert (nf1, nf2) == (kc['nFluidWith'], kc['nFluidWithout'])
+    assert rA['heatMW'] == pytest.approx(kc['heatMWwith'], rel=1e-12)
+    assert rB['heatMW'] == pytest.approx(kc['heatMWwithout'], rel=1e-12)
+    assert stA['nonFinite'] + stB['nonFinite'] == 0
+    assert max(stA['umax'], stB['umax']) == pytest.approx(kc['umaxDomain'], rel=2e-2)
+    s.setExistingFlux(800)
+    assert s.info['heatExistingMW'] == pytest.approx(k['heatExistingMW800'], rel=1e-12)
+    s.resetHeat()
+    rH = s.read().result()
+    assert rH['simTime'] == 0 and rH['thetaMax'] == 0
+    assert surf_stats(rH)['windMean'] == pytest.approx(k['afterResetHeat']['windMean'], rel=1e-3)
+    s.step(200).result()
+    s.resetFlow()
+    rF = s.read().result()
+    assert rF['simTime'] == 0 and rF['thetaMax'] == 0
+    assert surf_stats(rF)['windMean'] == pytest.approx(k['afterResetFlow']['windMean'], rel=1e-6)
+    s.setMet(dict(u10=4, dirFrom=230))
+    n1 = s.flowReinits
+    s.setMet(dict(u10=4, dirFrom=30))
+    n2 = s.flowReinits
+    assert dict(afterSmallTurn=n1, afterBigTurn=n2) == k['flowReinits']
+    s.destroy()
+    with pytest.raises(S.LiveSolverError) as e:
+        s.step(1).result()
+    assert 'rejected: ' + str(e.value) == k['afterDestroy']
+    # a caller-chosen device ordinal
+    s2 = real_solver(lambda nx, ny, nz: __import__('ashburn_heat_twin_b200.cuda_device', fromlist=['x'])
+                     .CudaDevice(nx, ny, nz, device=0), dx=40)
+    s2.step(100).result()
+    r2 = s2.read().result()
+    assert np.isfinite(r2['thetaMax'])
+    assert r2['simTime'] == pytest.approx(34.22293308116463, rel=1e-12)   # api20 ownDevice.simTime
+    s2.destroy()

@@ -1,0 +1,196 @@
+"""Parity of the CUDA path (libahx.so through the C ABI) with the CPU oracle on the same seeded inputs.
+
+Bar: the exact-arithmetic build (-fmad=false) is bit-identical to the oracle for the f32 state, the step outputs,
+the read-back and the FP64 build; the FMA build and the 16-bit storage formats are held to stated tolerances.
+"""
+import numpy as np
+import pytest
+
+from tests.helpers import cuda_backend, oracle_backend, rel_l2, small_solver
+
+pytestmark = pytest.mark.gpu
+
+# wind directions covering every inflow-face combination of the eps rule (solver.js:264-269):
+# 250 -> w s, 75 -> e n, 180 -> s only, 0 -> n only, 300 -> w n, 120 -> e s, 90 -> e only, 270 -> w only
+DIRS = [250.0, 75.0, 180.0, 0.0, 300.0, 120.0, 90.0, 270.0]
+
+
+def _pair(**kw):
+    g = small_solver(cuda_backend('fp32', 'exact'), **kw)
+    o = small_solver(oracle_backend(), **kw)
+    return g, o
+
+
+def _state_equal(g, o):
+    sg, so = g._dbg.readState(), o._dbg.readState()
+    return np.array_equal(sg['f'], so['f']) and np.array_equal(sg['g'], so['g'])
+
+
+@pytest.mark.parametrize('dirFrom', DIRS)
+@pytest.mark.parametrize('oclip', [True, False])
+def test_step_bit_exact(dirFrom, oclip):
+    met = dict(u10=5.0, dirFrom=dirFrom, wstar=1.5, blh=700.0)
+    g, o = _pair(met=met, outflowClip=oclip, nsw=6)
+    assert _state_equal(g, o), 'initial state differs'
+    for s in (g, o):
+        s._dbg.stepOut(7).result()
+    sg, so = g._dbg.readState(), o._dbg.readState()
+    assert np.array_equal(sg['f'], so['f']), f"f differs: {np.abs(sg['f'] - so['f']).max()}"
+    assert np.array_equal(sg['g'], so['g']), f"g differs: {np.abs(sg['g'] - so['g']).max()}"
+    assert np.array_equal(g._dbg.readDbg(), o._dbg.readDbg())
+    rg, ro = g.read().result(), o.read().result()
+    for key in ('surf', 'u', 'v', 'vol'):
+        assert np.array_equal(rg[key], ro[key]), key
+    assert rg['thetaMax'] == ro['thetaMax']
+    g.destroy()
+    o.destroy()
+
+
+def test_long_run_with_controls_bit_exact():
+    """Met changes (including a re-initialising turn), flux changes, a campus added and removed, resets and the
+    accumulation mode, all bit-identical to the oracle over 60 steps."""
+    g, o = _pair(met=dict(u10=3.0, dirFrom=210.0, wstar=1.67, blh=903.0))
+    campus = [dict(id='X', mw=80, halls=[[-2995 + 150, -2995 + 120, -2995 + 330, -2995 + 260]])]
+    script = [
+        ('step', 10), ('setMet', dict(u10=6.0, dirFrom=230.0)), ('step', 5), ('campus', campus), ('step', 8),
+        ('flux', 900), ('acc', 6), ('setMet', dict(u10=2.0, dirFrom=40.0)), ('step', 5), ('campus', []),
+        ('step', 7), ('resetHeat', None), ('step', 4), ('out', 3),
+    ]
+    for s in (g, o):
+        s._dbg.clearDbg()
+        for op, arg in script:
+            if op == 'step':
+                s.step(arg).result()
+            elif op == 'setMet':
+                s.setMet(arg)
+            elif op == 'campus':
+                s.setNewCampuses(arg)
+            elif op == 'flux':
+                s.setExistingFlux(arg)
+            elif op == 'acc':
+                s._dbg.stepAcc(arg).result()
+            elif op == 'out':
+                s._dbg.stepOut(arg).result()
+            elif op == 'resetHeat':
+                s.resetHeat()
+    assert g.flowReinits == o.flowReinits == 1
+    assert _state_equal(g, o)
+    assert np.array_equal(g._dbg.readDbg(), o._dbg.readDbg())
+    sg, so = g._dbg.stats(), o._dbg.stats()
+    assert sg['nonFinite'] == so['nonFinite'] == 0
+    assert sg['nFluid'] == so['nFluid']
+    assert sg['thetaMax'] == so['thetaMax'] and sg['umax'] == so['umax']
+    for key in ('heatContentMJ', 'keMean', 'rhoDevMean'):
+        assert sg[key] == pytest.approx(so[key], rel=1e-12, abs=1e-18)
+    g.destroy()
+    o.destroy()
+
+
+def test_write_state_roundtrip_and_step():
+    """A state written through the C ABI (the reference's _dbg.writeState) steps identically on both sides."""
+    g, o = _pair()
+    rng = np.random.default_rng(3)
+    N = g.info['nCells']
+    w = np.array([1 / 3] + [1 / 18] * 6 + [1 / 36] * 12, np.float32)
+    f = (np.repeat(w, N) * (1 + 0.02 * rng.standard_normal(19 * N))).astype(np.float32)
+    gg = (0.1 * rng.random(7 * N)).astype(np.float32)
+    for s in (g, o):
+        s._dbg.writeState(f, gg)
+    st = g._dbg.readState()
+    assert np.array_equal(st['f'], f) and np.array_equal(st['g'], gg)
+    for s in (g, o):
+        s.step(3).result()
+    assert _state_equal(g, o)
+    g.destroy()
+    o.destroy()
+
+
+def test_fast_arithmetic_within_tolerance():
+    """The FMA-contracted build: single-step theta rel-L2 <= 1e-5 against the oracle (the north-star parity bar),
+    and <= 1e-4 after 200 steps."""
+    met = dict(u10=5.0, dirFrom=250.0, wstar=1.5, blh=700.0)
+    f = small_solver(cuda_backend('fp32', 'fast'), met=met)
+    o = small_solver(oracle_backend(), met=met)
+    for s in (f, o):
+        s.step(50).result()
+    # one step from an identical state
+    st = o._dbg.readState()
+    f._dbg.writeState(st['f'], st['g'])
+    for s in (f, o):
+        s._dbg.stepOut(1).result()
+    a, b = f._dbg.readDbg().reshape(-1, 4), o._dbg.readDbg().reshape(-1, 4)
+    fl = b[:, 0] != 0
+    assert rel_l2(a[fl, 0], b[fl, 0]) <= 1e-5
+    assert rel_l2(a[fl, 1], b[fl, 1]) <= 1e-5
+    for s in (f, o):
+        s._dbg.stepOut(200).result()
+    a, b = f._dbg.readDbg().reshape(-1, 4), o._dbg.readDbg().reshape(-1, 4)
+    assert rel_l2(a[:, 0], b[:, 0]) <= 1e-4
+    f.destroy()
+    o.destroy()
+
+
+def test_fp64_build_bit_exact_with_fp64_oracle():
+    met = dict(u10=4.0, dirFrom=300.0, wstar=1.0, blh=800.0)
+    g = small_solver(cuda_backend('fp64', 'exact'), met=met)
+    o = small_solver(oracle_backend(np.float64), met=met)
+    for s in (g, o):
+        s.step(9).result()
+    fg, gg = g._dev.read_state_f64()
+    fo, go = o._dev.read_state()
+    assert np.array_equal(fg, fo) and np.array_equal(gg, go)
+    g.destroy()
+    o.destroy()
+
+
+@pytest.mark.parametrize('precision,tol', [('fp16', 2e-3), ('bf16', 2e-2)])
+def test_16bit_storage_error_vs_fp64(precision, tol):
+    """16-bit population storage (shifted by w_q, scaled) against the FP64 build after 300 steps with heat on:
+    theta rel-L2 over fluid cells within the stated tolerance."""
+    met = dict(u10=5.0, dirFrom=250.0, wstar=1.5, blh=700.0)
+    h = small_solver(cuda_backend(precision, 'exact'), met=met)
+    d = small_solver(cuda_backend('fp64', 'exact'), met=met)
+    for s in (h, d):
+        s._dbg.stepOut(300).result()
+    a, b = h._dbg.readDbg().reshape(-1, 4), d._dbg.readDbg().reshape(-1, 4)
+    fl = b[:, 0] != 0
+    err = rel_l2(a[fl, 0], b[fl, 0])
+    assert err <= tol, err
+    assert np.isfinite(a).all()
+    h.destroy()
+    d.destroy()
+
+
+def test_budget_record_matches_step_outputs():
+    """The fused FP64 budget sums equal the same sums taken over the step's out-mode fields."""
+    g = small_solver(cuda_backend('fp32', 'exact'), met=dict(u10=5.0, dirFrom=250.0, wstar=1.5, blh=700.0))
+    g.step(20).result()
+    g._dev.budget_enable(True)
+    g._dev.budget_read(reset=True)
+    g._dbg.stepOut(1).result()
+    b = g._dev.budget_read(reset=True)
+    g._dev.budget_enable(False)
+    nx, ny, nz = g.info['nx'], g.info['ny'], g.info['nz']
+    dbg = g._dbg.readDbg().reshape(nz, ny, nx, 4).astype(np.float64)
+    ktop = g._ktopS.reshape(ny, nx)
+    fluid = np.arange(nz)[:, None, None] >= ktop[None]
+    th, ux, uy = dbg[..., 0], dbg[..., 1], dbg[..., 2]
+    assert b['cells'] == fluid.sum()
+    assert b['theta_sum'] == pytest.approx((th * fluid).sum(), rel=1e-6)
+    assert b['src_sum'] == pytest.approx(float(g._q.astype(np.float64).sum()), rel=1e-6)
+    faces = [(th * ux)[:, :, 0], (th * ux)[:, :, -1], (th * uy)[:, 0, :], (th * uy)[:, -1, :]]
+    fmask = [fluid[:, :, 0], fluid[:, :, -1], fluid[:, 0, :], fluid[:, -1, :]]
+    for a in range(4):
+        assert b['face_theta_u'][a] == pytest.approx((faces[a] * fmask[a]).sum(), rel=1e-5, abs=1e-9)
+    g.destroy()
+
+
+def test_autotune_keeps_state():
+    g, o = _pair()
+    by, zs, ms = g._dev.autotune(2)
+    assert by in (2, 4, 8) and zs >= 1 and ms > 0
+    for s in (g, o):
+        s.step(4).result()
+    assert _state_equal(g, o)
+    g.destroy()
+    o.destroy()
