@@ -15,7 +15,7 @@
 #include <thread>
 #include <vector>
 
-#include "../../include/ahx.h"
+#include "ahx.h"
 #include "launch.h"
 
 using namespace ahx;

@@ -114,7 +114,9 @@ __global__ void __launch_bounds__(256) vol_kernel(DomainView D, int nzv, float v
             } else if (sk < (int)__ldg(D.ktop + (long)sj * nx + si)) {
               gv = K::dec_g(K::load(gA + (uint32_t)opp7(q) * D.qs + n));
             } else {
-              gv = K::dec_g(K::load(gA + (uint32_t)q * D.qs + n - (uint32_t)(cx + cy * D.px + cz * (int)D.ps)));
+              // the offset wraps in 32 bits before it touches the pointer (cx = -1 gives a negative shift)
+              const uint32_t off = (uint32_t)q * D.qs + n - (uint32_t)(cx + cy * D.px + cz * (int)D.ps);
+              gv = K::dec_g(K::load(gA + off));
             }
             g[q] = gv;
           });
