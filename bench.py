@@ -29,7 +29,12 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-WORKLOAD = '600x600x64 cells at 10 m (23.04 M), synthetic seed 2: 24 hills 0-40 m, 4000 buildings, 211 DC roofs'
+WORKLOADS = {
+    'c2': dict(desc='600x600x64 cells at 10 m (23.04 M), synthetic seed 2: 24 hills 0-40 m, 4000 buildings, '
+                    '211 DC roofs', dx=10, heightM=640, met='C2_MET', spec='C2'),
+    'c1': dict(desc='200x200x32 cells at 30 m (1.28 M), synthetic seed 1: 8 hills 0-30 m, 1500 buildings, '
+                    '60 DC roofs', dx=30, heightM=960, met='C1_MET', spec='C1'),
+}
 METRIC = 'GLUPS (all cells) of the fused D3Q19+D3Q7 step, 600x600x64'
 
 
@@ -37,12 +42,13 @@ def log(*a):
     print(*a, file=sys.stderr, flush=True)
 
 
-def make_solver(backend=None, device=None, precision='fp32', arith='exact'):
+def make_solver(backend=None, device=None, precision='fp32', arith='exact', workload='c2'):
     from ashburn_heat_twin_b200 import solver as S
     from ashburn_heat_twin_b200 import synth
-    st = synth.make_static10(synth.C2)
-    kw = dict(static=st, dx=10, allowAnyDx=True, heightM=640, u10Max=8, alpha=0.2, met=synth.C2_MET,
-              existingFlux=400)
+    w = WORKLOADS[workload]
+    st = synth.make_static10(getattr(synth, w['spec']))
+    kw = dict(static=st, dx=w['dx'], allowAnyDx=True, heightM=w['heightM'], u10Max=8, alpha=0.2,
+              met=getattr(synth, w['met']), existingFlux=400)
     if backend is None:
         from ashburn_heat_twin_b200.cuda_device import CudaDevice
 
@@ -152,7 +158,7 @@ def run_reference(a, rank):
     out = dict(metric=METRIC, value=v, unit='GLUPS', n_gpus=a.gpus, steps=a.steps, warmup=a.warmup,
                ms_per_step=t / a.steps * 1e3, higher_is_better=True, scaling='weak', vs_baseline=None, dtype='f32',
                data='synthetic', impl='reference',
-               config=dict(workload=WORKLOAD, precision='fp32', scheme='pull', parallelism='replicas'),
+               config=dict(workload=WORKLOADS['c2']['desc'], precision='fp32', scheme='pull', parallelism='replicas'),
                cpu_baseline=dict(value=v, unit='GLUPS', cores=O.max_threads(), kind='port',
                                  sample=f'{a.steps} full steps after {a.warmup} warm-up steps'),
                e2e=dict(value=v, unit='GLUPS', h2d_bytes_per_step=0, d2h_bytes_per_step=0))
@@ -173,6 +179,8 @@ def main():
     ap.add_argument('--frame', type=int, default=10, help='steps per e2e frame (setMet + step(F) + read())')
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--no-autotune', action='store_true')
+    ap.add_argument('--workload', default='c2', choices=sorted(WORKLOADS),
+                    help='c2 (the benchmark) or c1 (a smaller case for profiling)')
     a = ap.parse_args()
     a.warmup = max(a.warmup, 3)
 
@@ -193,7 +201,7 @@ def main():
                                 device_id=torch.device('cuda', local))
     from ashburn_heat_twin_b200 import _build
     _build.build()
-    s = make_solver(device=local, precision=a.precision, arith=a.arith)
+    s = make_solver(device=local, precision=a.precision, arith=a.arith, workload=a.workload)
     dev = s._dev
     nx, ny, nz = s.info['nx'], s.info['ny'], s.info['nz']
     cells = nx * ny * nz
@@ -270,12 +278,13 @@ def main():
         s_steps = s._steps
         cpu = cpu_baseline()
         del s_steps
-    out = dict(metric=METRIC, value=value, unit='GLUPS', n_gpus=world, steps=a.steps, warmup=a.warmup,
+    metric = METRIC if a.workload == 'c2' else METRIC.replace('600x600x64', '200x200x32')
+    out = dict(metric=metric, value=value, unit='GLUPS', n_gpus=world, steps=a.steps, warmup=a.warmup,
                ms_per_step=ms_all / a.steps, higher_is_better=True, scaling='weak', vs_baseline=None,
                dtype={'fp32': 'f32', 'fp16': 'f16-store/f32', 'bf16': 'bf16-store/f32', 'fp64': 'f64'}[a.precision],
                data='synthetic (seeded terrain and buildings; no public dataset involved)',
-               config=dict(workload=WORKLOAD, precision=a.precision, arith=a.arith, scheme='pull',
-                           parallelism=f'replicas x{world}', fluid_cells=fluid, l2='state 4.8 GB >> 126 MB L2',
+               config=dict(workload=WORKLOADS[a.workload]['desc'], precision=a.precision, arith=a.arith, scheme='pull',
+                           parallelism=f'replicas x{world}', fluid_cells=fluid, l2=f"state {s._dev.info()['state_bytes'] / 1e9:.2f} GB vs 126 MB L2",
                            launch=dict(block_y=tune[0], zslab=tune[1]) if tune else None),
                roofline=roof, cpu_baseline=cpu, e2e=e2e, gpu_launches=a.steps, clocks=clocks,
                glups_fluid=world * fluid * a.steps / (ms_all / 1e3) / 1e9)
