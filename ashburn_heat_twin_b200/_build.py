@@ -3,10 +3,12 @@
 Translation units and their arithmetic flags:
   step_exact.cu  -fmad=false  fused step, every f32 expression individually rounded (bit-identical to the CPU
                               restatement of the reference kernels)
-  step_fast.cu   -fmad=true   fused step with multiply-add contraction
+  step_fast.cu   -fmad=true   fused step with multiply-add contraction, approximate division and square root and
+                              the paired collision
   aux.cu         -fmad=false  read-back, init, re-init, stats, layout conversion
   api.cu                      the C ABI (include/ahx.h)
-All use -ftz=true (f32 subnormals flushed, as the CPU restatement does) with IEEE division and square root.
+All use -ftz=true (f32 subnormals flushed, as the CPU restatement does); all but step_fast.cu use IEEE division and
+square root.
 """
 from __future__ import annotations
 
@@ -24,13 +26,14 @@ LIB = os.path.join(HERE, 'libahx.so')
 OBJDIR = os.path.join(HERE, '_build')
 
 ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
-COMMON = ['-O3', '-std=c++17', '--expt-relaxed-constexpr', '-lineinfo', '-ftz=true', '-prec-div=true',
-          '-prec-sqrt=true', '-Xcompiler', '-fPIC', '-I', INCLUDE]
+COMMON = ['-O3', '-std=c++17', '--expt-relaxed-constexpr', '-lineinfo', '-ftz=true', '-Xcompiler', '-fPIC', '-I',
+          INCLUDE]
+IEEE = ['-prec-div=true', '-prec-sqrt=true']
 UNITS = {
-    'step_exact.cu': ['-fmad=false'],
-    'step_fast.cu': ['-fmad=true'],
-    'aux.cu': ['-fmad=false'],
-    'api.cu': ['-fmad=false'],
+    'step_exact.cu': ['-fmad=false'] + IEEE,
+    'step_fast.cu': ['-fmad=true', '-prec-div=false', '-prec-sqrt=false'],
+    'aux.cu': ['-fmad=false'] + IEEE,
+    'api.cu': ['-fmad=false'] + IEEE,
 }
 
 

@@ -82,6 +82,7 @@ struct Column {
   bool face;             // on any lateral face: some sources are outside the domain
   bool spon;             // inside the outflow viscous sponge (kernel.js:322-330)
   R spg;                 // 0.15*rr*rr of the sponge
+  int kint;              // first level whose whole 3x3x3 neighbourhood is fluid (interior fast path from here)
 };
 
 template <class R>
@@ -101,6 +102,12 @@ __device__ __forceinline__ void load_column(const DomainView& D, const ParamsHea
 #pragma unroll
     for (int oy = 0; oy < 3; ++oy)
       C.kn[ox][oy] = (ox == 1 && oy == 1) ? C.kg : (int)__ldg(D.ktop + (size_t)ys[oy] * nx + xs[ox]);
+  int km = C.kg;
+#pragma unroll
+  for (int ox = 0; ox < 3; ++ox)
+#pragma unroll
+    for (int oy = 0; oy < 3; ++oy) km = max(km, C.kn[ox][oy]);
+  C.kint = km + 1;
   C.latW = (i == 0);
   C.latE = (i == nx - 1);
   C.latS = (j == 0);
@@ -269,6 +276,38 @@ __device__ __forceinline__ void stream_cell(const DomainView& D, const ParamsHea
   }
 }
 
+// Interior cells (not on a lateral face, below the lid, every source fluid): the stream is a plain gather, one load
+// per population at a fixed offset; loads exactly the values stream_cell would.
+template <class S>
+__device__ __forceinline__ void stream_interior(const DomainView& D, const float4* prof,
+                                                const Column<typename Codec<S>::Real>& C, int k, uint32_t n,
+                                                Cell<typename Codec<S>::Real>& X) {
+  using R = typename Codec<S>::Real;
+  using K = Codec<S>;
+  const S* fA = static_cast<const S*>(D.fA);
+  const S* gA = static_cast<const S*>(D.gA);
+  const uint32_t qs = D.qs, ps = D.ps, px = (uint32_t)D.px;
+  int zagl = k - C.ktc;
+  if (zagl < 0) zagl = 0;
+  if (zagl > D.nz - 1) zagl = D.nz - 1;
+  const float4 pr = prof[zagl];
+  X.uI = R(pr.x);
+  X.vI = R(pr.y);
+  X.kb = R(pr.z);
+  static_for<19>([&](auto Q) {
+    constexpr int q = Q;
+    constexpr int cx = kC19[q][0], cy = kC19[q][1], cz = kC19[q][2];
+    const uint32_t off = (uint32_t)q * qs + n - (uint32_t)(cx + cy * (int)px + cz * (int)ps);
+    X.f[q] = K::dec_f(K::load(fA + off), R(w19(q)));
+  });
+  static_for<7>([&](auto Q) {
+    constexpr int q = Q;
+    constexpr int cx = kC7[q][0], cy = kC7[q][1], cz = kC7[q][2];
+    const uint32_t off = (uint32_t)q * qs + n - (uint32_t)(cx + cy * (int)px + cz * (int)ps);
+    X.g[q] = K::dec_g(K::load(gA + off));
+  });
+}
+
 template <class R>
 struct Macro {
   R rho, jx, jy, jz, th;
@@ -396,6 +435,136 @@ __device__ __forceinline__ void collide_store(const DomainView& D, const ParamsH
   });
 }
 
+// The same relaxation in the contracted build, rearranged: each population q is paired with its opposite (adjacent
+// in the velocity table), the even and odd parts of the equilibrium, the regularised non-equilibrium term (even in c)
+// and the Guo forcing are formed once per pair, and 1/rho, 1/tau are taken once. Mathematically identical to
+// moments_forces + collide_store; rounding differs (held to the single-step theta rel-L2 <= 1e-5 bar).
+template <class S>
+__device__ __forceinline__ void fast_update(const DomainView& D, const ParamsHead& P,
+                                            const Column<typename Codec<S>::Real>& C, int k, uint32_t n,
+                                            const Cell<typename Codec<S>::Real>& X,
+                                            Macro<typename Codec<S>::Real>& M) {
+  using R = typename Codec<S>::Real;
+  using K = Codec<S>;
+  S* fB = static_cast<S*>(D.fB);
+  S* gB = static_cast<S*>(D.gB);
+  const uint32_t qs = D.qs;
+  R sp9[9], dp9[9];
+  static_for<9>([&](auto Pi) {
+    constexpr int p = Pi;
+    sp9[p] = X.f[2 * p + 1] + X.f[2 * p + 2];
+    dp9[p] = X.f[2 * p + 1] - X.f[2 * p + 2];
+  });
+  R rho = X.f[0];
+#pragma unroll
+  for (int p = 0; p < 9; ++p) rho += sp9[p];
+  R jx = R(0), jy = R(0), jz = R(0), Pxx = R(0), Pyy = R(0), Pzz = R(0), Pxy = R(0), Pxz = R(0), Pyz = R(0);
+  static_for<9>([&](auto Pi) {
+    constexpr int p = Pi;
+    constexpr int q = 2 * p + 1;
+    constexpr int cx = kC19[q][0], cy = kC19[q][1], cz = kC19[q][2];
+    if constexpr (cx != 0) { jx += R(cx) * dp9[p]; Pxx += sp9[p]; }
+    if constexpr (cy != 0) { jy += R(cy) * dp9[p]; Pyy += sp9[p]; }
+    if constexpr (cz != 0) { jz += R(cz) * dp9[p]; Pzz += sp9[p]; }
+    if constexpr (cx != 0 && cy != 0) Pxy += R(cx * cy) * sp9[p];
+    if constexpr (cx != 0 && cz != 0) Pxz += R(cx * cz) * sp9[p];
+    if constexpr (cy != 0 && cz != 0) Pyz += R(cy * cz) * sp9[p];
+  });
+  const R th = X.g[0] + (X.g[1] + X.g[2]) + (X.g[3] + X.g[4]) + (X.g[5] + X.g[6]);
+  const R irho = R(1) / rho;
+  R Fx = R(0), Fy = R(0), Fz = rho * R(P.gbeta) * th;
+  if (k == C.kg && C.kg == C.ktc) {
+    const R ux0 = jx * irho, uy0 = jy * irho;
+    const R sp = sqrt(ux0 * ux0 + uy0 * uy0);
+    const R cd = R(C.cd);
+    const R a = (cd * sp > R(0.5)) ? R(-0.5) * rho : -rho * cd * sp;   // implicit-limited log-law drag
+    Fx = a * ux0;
+    Fy = a * uy0;
+  }
+  R sg = R(0);
+  if (k >= D.nz - P.nsp) {
+    const R aa = (R(k - (D.nz - P.nsp)) + R(1.0)) / R(P.nsp);
+    sg = R(P.sigmax) * aa * aa;
+    const R rs = rho * sg;
+    Fx += rs * (X.uI - jx * irho);
+    Fy += rs * (X.vI - jy * irho);
+    Fz -= rs * (jz * irho);
+  }
+  const R ux = (jx + R(0.5) * Fx) * irho, uy = (jy + R(0.5) * Fy) * irho, uz = (jz + R(0.5) * Fz) * irho;
+  const R usq = ux * ux + uy * uy + uz * uz;
+  const R r3 = rho * R(1.0 / 3.0);
+  const R Nxx = Pxx - r3 - rho * ux * ux;
+  const R Nyy = Pyy - r3 - rho * uy * uy;
+  const R Nzz = Pzz - r3 - rho * uz * uz;
+  const R Nxy = Pxy - rho * ux * uy;
+  const R Nxz = Pxz - rho * ux * uz;
+  const R Nyz = Pyz - rho * uy * uz;
+  const R Pn = sqrt(Nxx * Nxx + Nyy * Nyy + Nzz * Nzz + R(2.0) * (Nxy * Nxy + Nxz * Nxz + Nyz * Nyz));
+  R tb = R(P.tau0) + R(3.0) * R(P.momfac) * X.kb;
+  if (C.spon) tb += C.spg;
+  const R tau = R(0.5) * (tb + sqrt(tb * tb + R(P.cs2smag) * Pn * irho));
+  const R itau = R(1) / tau;
+  const R nusgs = (tau - tb) * R(1.0 / 3.0);
+  const R kap = nusgs / R(P.prt) + X.kb + R(P.kfloor);
+  const R taug = R(0.5) + R(4.0) * kap;
+  const R om = R(1.0) - itau;
+  const R fpre = R(1.0) - R(0.5) * itau;
+  const R trN = (Nxx + Nyy + Nzz) * R(1.0 / 3.0);
+  const R uF = ux * Fx + uy * Fy + uz * Fz;
+  const R base = R(1.0) - R(1.5) * usq;
+  // q = 0
+  {
+    const R w = R(w19(0));
+    const R f0 = w * rho * base + om * R(4.5 * w19(0)) * (-trN) + fpre * w * (R(-3.0) * uF);
+    __stcs(fB + n, K::enc_f(f0, w));
+  }
+  static_for<9>([&](auto Pi) {
+    constexpr int p = Pi;
+    constexpr int q = 2 * p + 1;
+    constexpr int cx = kC19[q][0], cy = kC19[q][1], cz = kC19[q][2];
+    const R w = R(w19(q));
+    const R cu = cdot<R, cx, cy, cz>(ux, uy, uz);
+    const R cF = cdot<R, cx, cy, cz>(Fx, Fy, Fz);
+    R qn = R(0);
+    if constexpr (cx != 0) qn += Nxx;
+    if constexpr (cy != 0) qn += Nyy;
+    if constexpr (cz != 0) qn += Nzz;
+    if constexpr (cx != 0 && cy != 0) qn += R(2 * cx * cy) * Nxy;
+    if constexpr (cx != 0 && cz != 0) qn += R(2 * cx * cz) * Nxz;
+    if constexpr (cy != 0 && cz != 0) qn += R(2 * cy * cz) * Nyz;
+    const R rw = rho * w, fw = fpre * w;
+    const R E = rw * (base + R(4.5) * cu * cu) + om * R(4.5 * w19(q)) * (qn - trN) + fw * (R(9.0) * cu * cF - R(3.0) * uF);
+    const R O = R(3.0) * (rw * cu + fw * cF);
+    __stcs(fB + (uint32_t)q * qs + n, K::enc_f(E + O, w));
+    __stcs(fB + (uint32_t)(q + 1) * qs + n, K::enc_f(E - O, w));
+  });
+  const R Ssrc = (k == C.kg) ? R(C.qsrc) * R(P.srcscale) : R(0);
+  const R omg = R(1.0) / taug;
+  const R a = R(1.0) - omg, one_sg = R(1.0) - sg;
+  __stcs(gB + n, K::enc_g((a * X.g[0] + omg * R(w7(0)) * th + R(w7(0)) * Ssrc) * one_sg));
+  static_for<3>([&](auto Pi) {
+    constexpr int p = Pi;
+    constexpr int q = 2 * p + 1;
+    constexpr int cx = kC7[q][0], cy = kC7[q][1], cz = kC7[q][2];
+    const R b = omg * R(w7(q)) * th + R(w7(q)) * Ssrc;
+    const R c4 = omg * R(4.0 * w7(q)) * th * cdot<R, cx, cy, cz>(ux, uy, uz);
+    __stcs(gB + (uint32_t)q * qs + n, K::enc_g((a * X.g[q] + b + c4) * one_sg));
+    __stcs(gB + (uint32_t)(q + 1) * qs + n, K::enc_g((a * X.g[q + 1] + b - c4) * one_sg));
+  });
+  M.rho = rho;
+  M.jx = jx;
+  M.jy = jy;
+  M.jz = jz;
+  M.th = th;
+  M.Fx = Fx;
+  M.Fy = Fy;
+  M.Fz = Fz;
+  M.sg = sg;
+  M.ux = ux;
+  M.uy = uy;
+  M.uz = uz;
+}
+
 // Budget accumulators of one thread (summed over its cells, then reduced per block into FP64).
 struct BudgetAcc {
   float theta, src, cells;
@@ -405,7 +574,7 @@ struct BudgetAcc {
 constexpr int kBlockX = 32;
 
 // The fused step over one z-slab of the columns of a block. MODE: 0 none, 1 write dbg, 2 accumulate dbg.
-template <class S, int MODE, bool BUDGET>
+template <class S, int MODE, bool BUDGET, bool FAST>
 __device__ __forceinline__ void step_block(const DomainView& D, int bx, int by, int bz, int zslab) {
   using R = typename Codec<S>::Real;
   extern __shared__ float4 smem_prof[];
@@ -435,10 +604,15 @@ __device__ __forceinline__ void step_block(const DomainView& D, int bx, int by, 
     for (int k = max(k0, C.kg); k < k1; ++k) {
       const uint32_t n = (uint32_t)k * D.ps + base;
       Cell<R> X;
-      stream_cell<S>(D, P, smem_prof, C, k, n, X);
+      if (!C.face && k >= C.kint && k < D.nz - 1) stream_interior<S>(D, smem_prof, C, k, n, X);
+      else stream_cell<S>(D, P, smem_prof, C, k, n, X);
       Macro<R> M;
-      moments_forces<R>(P, C, k, D.nz, X, M);
-      collide_store<S>(D, P, C, k, n, X, M);
+      if constexpr (FAST) {
+        fast_update<S>(D, P, C, k, n, X, M);
+      } else {
+        moments_forces<R>(P, C, k, D.nz, X, M);
+        collide_store<S>(D, P, C, k, n, X, M);
+      }
       if constexpr (MODE == 1) {
         D.dbg[n] = make_float4((float)M.th, (float)M.ux, (float)M.uy, (float)M.uz);
       } else if constexpr (MODE == 2) {

@@ -9,9 +9,13 @@
 namespace ahx {
 namespace AHX_STEP_NS {
 
+#ifndef AHX_STEP_FAST
+#define AHX_STEP_FAST 0
+#endif
+
 template <class S, int MODE, bool BUDGET>
 __global__ void __launch_bounds__(256) step_kernel(DomainView D, int zslab) {
-  step_block<S, MODE, BUDGET>(D, blockIdx.x, blockIdx.y, blockIdx.z, zslab);
+  step_block<S, MODE, BUDGET, AHX_STEP_FAST != 0>(D, blockIdx.x, blockIdx.y, blockIdx.z, zslab);
 }
 
 template <class S, int MODE, bool BUDGET>
