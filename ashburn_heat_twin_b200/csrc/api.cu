@@ -82,7 +82,7 @@ struct ahx_handle {
   StatsScratch* d_stats = nullptr;
   int parity = 0;
   int64_t steps = 0;
-  int block_y = 4, zslab = 0;
+  int block_y = 4, zslab = 0, minb = 0;
   ReadSlot reads[AHX_MAX_READS];
   uint64_t next_read = 0;
   UploadSlot up[kUploadSlots];
@@ -138,6 +138,7 @@ DomainView view(ahx_handle* h) {
   D.px = h->px;
   D.ps = h->ps;
   D.qs = h->qs;
+  set_offsets(D);
   return D;
 }
 
@@ -432,6 +433,7 @@ ahx_status ahx_step(ahx_handle* h, int n, int mode) {
   L.budget = h->budget_on;
   L.block_y = h->block_y;
   L.zslab = h->zslab;
+  L.minb = h->minb;
   for (int s = 0; s < n; ++s) {
     L.mode = (mode == AHX_MODE_ACC) ? 2 : ((mode == AHX_MODE_OUT && s == n - 1) ? 1 : 0);
     DomainView D = view(h);
@@ -742,8 +744,13 @@ ahx_status ahx_set_launch(ahx_handle* h, int block_y, int zslab) {
   if (!h) return fail(AHX_EINVAL, "live solver: null handle");
   std::lock_guard<std::mutex> lk(h->mu);
   if (ahx_status st = check(h)) return st;
-  if (block_y < 0 || block_y > 8 || zslab < 0) return fail(AHX_EINVAL, "live solver: bad launch shape");
-  if (block_y) h->block_y = block_y;
+  const int by = block_y % 100, mb = block_y / 100;
+  if (by < 0 || by > 8 || zslab < 0 || (mb != 0 && (mb < 4 || mb > 6)) || (mb && by != 4))
+    return fail(AHX_EINVAL, "live solver: bad launch shape");
+  if (block_y) {
+    h->block_y = by;
+    h->minb = mb;
+  }
   if (zslab) h->zslab = zslab;
   return AHX_OK;
 }
@@ -771,10 +778,13 @@ ahx_status ahx_autotune(ahx_handle* h, int steps_per_trial, int* best_block_y, i
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
-  const int bys[] = {2, 4, 8};
+  struct Shape {
+    int by, minb;
+  };
+  const Shape shapes[] = {{2, 0}, {4, 0}, {8, 0}, {4, 4}, {4, 5}, {4, 6}};
   std::vector<int> zss = {h->dims.nz, 32, 16, 8};
   float best = 1e30f;
-  int bby = h->block_y, bzs = h->zslab;
+  int bby = h->block_y, bzs = h->zslab, bmb = h->minb;
   DomainView D = view(h);
   D.dbg = nullptr;
   StepLaunch L;
@@ -782,10 +792,11 @@ ahx_status ahx_autotune(ahx_handle* h, int steps_per_trial, int* best_block_y, i
   L.mode = 0;
   L.budget = false;
   ahx_status st = AHX_OK;
-  for (int by : bys) {
+  for (const Shape& sh : shapes) {
     for (int zs : zss) {
       if (zs > h->dims.nz) continue;
-      L.block_y = by;
+      L.block_y = sh.by;
+      L.minb = sh.minb;
       L.zslab = zs;
       float ms = 0;
       for (int rep = 0; rep < 2 && st == AHX_OK; ++rep) {   // rep 0 warms up
@@ -810,8 +821,9 @@ ahx_status ahx_autotune(ahx_handle* h, int steps_per_trial, int* best_block_y, i
       ms /= steps_per_trial;
       if (ms < best) {
         best = ms;
-        bby = by;
+        bby = sh.by;
         bzs = zs;
+        bmb = sh.minb;
       }
     }
   }
@@ -825,7 +837,8 @@ ahx_status ahx_autotune(ahx_handle* h, int steps_per_trial, int* best_block_y, i
   if (st != AHX_OK) return st;
   h->block_y = bby;
   h->zslab = bzs;
-  if (best_block_y) *best_block_y = bby;
+  h->minb = bmb;
+  if (best_block_y) *best_block_y = bby * 100 + bmb;   // block_y, and the register-budget variant in the hundreds
   if (best_zslab) *best_zslab = bzs;
   if (best_ms) *best_ms = best;
   return AHX_OK;

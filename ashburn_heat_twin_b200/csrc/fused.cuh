@@ -286,7 +286,6 @@ __device__ __forceinline__ void stream_interior(const DomainView& D, const float
   using K = Codec<S>;
   const S* fA = static_cast<const S*>(D.fA);
   const S* gA = static_cast<const S*>(D.gA);
-  const uint32_t qs = D.qs, ps = D.ps, px = (uint32_t)D.px;
   int zagl = k - C.ktc;
   if (zagl < 0) zagl = 0;
   if (zagl > D.nz - 1) zagl = D.nz - 1;
@@ -296,15 +295,11 @@ __device__ __forceinline__ void stream_interior(const DomainView& D, const float
   X.kb = R(pr.z);
   static_for<19>([&](auto Q) {
     constexpr int q = Q;
-    constexpr int cx = kC19[q][0], cy = kC19[q][1], cz = kC19[q][2];
-    const uint32_t off = (uint32_t)q * qs + n - (uint32_t)(cx + cy * (int)px + cz * (int)ps);
-    X.f[q] = K::dec_f(K::load(fA + off), R(w19(q)));
+    X.f[q] = K::dec_f(K::load(fA + (n + D.pull_f[q])), R(w19(q)));
   });
   static_for<7>([&](auto Q) {
     constexpr int q = Q;
-    constexpr int cx = kC7[q][0], cy = kC7[q][1], cz = kC7[q][2];
-    const uint32_t off = (uint32_t)q * qs + n - (uint32_t)(cx + cy * (int)px + cz * (int)ps);
-    X.g[q] = K::dec_g(K::load(gA + off));
+    X.g[q] = K::dec_g(K::load(gA + (n + D.pull_g[q])));
   });
 }
 
@@ -421,7 +416,7 @@ __device__ __forceinline__ void collide_store(const DomainView& D, const ParamsH
     const R fr = w45 * (qn - trN);
     const R cF = cdot<R, cx, cy, cz>(Fx, Fy, Fz);
     const R Fq = fpre * w * (R(3.0) * (cF - uF) + R(9.0) * cu * cF);
-    __stcs(fB + (uint32_t)q * qs + n, K::enc_f(feq + om * fr + Fq, w));
+    K::store(fB + (n + D.plane[q]), K::enc_f(feq + om * fr + Fq, w));
   });
   R Ssrc = R(0);
   if (k == C.kg) Ssrc = R(C.qsrc) * R(P.srcscale);
@@ -431,7 +426,7 @@ __device__ __forceinline__ void collide_store(const DomainView& D, const ParamsH
     constexpr int cx = kC7[q][0], cy = kC7[q][1], cz = kC7[q][2];
     const R w = R(w7(q));
     const R geq = w * M.th * (R(1.0) + R(4.0) * cdot<R, cx, cy, cz>(ux, uy, uz));
-    __stcs(gB + (uint32_t)q * qs + n, K::enc_g((X.g[q] + omg * (geq - X.g[q]) + w * Ssrc) * (R(1.0) - M.sg)));
+    K::store(gB + (n + D.plane[q]), K::enc_g((X.g[q] + omg * (geq - X.g[q]) + w * Ssrc) * (R(1.0) - M.sg)));
   });
 }
 
@@ -516,7 +511,7 @@ __device__ __forceinline__ void fast_update(const DomainView& D, const ParamsHea
   {
     const R w = R(w19(0));
     const R f0 = w * rho * base + om * R(4.5 * w19(0)) * (-trN) + fpre * w * (R(-3.0) * uF);
-    __stcs(fB + n, K::enc_f(f0, w));
+    K::store(fB + n, K::enc_f(f0, w));
   }
   static_for<9>([&](auto Pi) {
     constexpr int p = Pi;
@@ -535,21 +530,21 @@ __device__ __forceinline__ void fast_update(const DomainView& D, const ParamsHea
     const R rw = rho * w, fw = fpre * w;
     const R E = rw * (base + R(4.5) * cu * cu) + om * R(4.5 * w19(q)) * (qn - trN) + fw * (R(9.0) * cu * cF - R(3.0) * uF);
     const R O = R(3.0) * (rw * cu + fw * cF);
-    __stcs(fB + (uint32_t)q * qs + n, K::enc_f(E + O, w));
-    __stcs(fB + (uint32_t)(q + 1) * qs + n, K::enc_f(E - O, w));
+    K::store(fB + (n + D.plane[q]), K::enc_f(E + O, w));
+    K::store(fB + (n + D.plane[q + 1]), K::enc_f(E - O, w));
   });
   const R Ssrc = (k == C.kg) ? R(C.qsrc) * R(P.srcscale) : R(0);
   const R omg = R(1.0) / taug;
   const R a = R(1.0) - omg, one_sg = R(1.0) - sg;
-  __stcs(gB + n, K::enc_g((a * X.g[0] + omg * R(w7(0)) * th + R(w7(0)) * Ssrc) * one_sg));
+  K::store(gB + n, K::enc_g((a * X.g[0] + omg * R(w7(0)) * th + R(w7(0)) * Ssrc) * one_sg));
   static_for<3>([&](auto Pi) {
     constexpr int p = Pi;
     constexpr int q = 2 * p + 1;
     constexpr int cx = kC7[q][0], cy = kC7[q][1], cz = kC7[q][2];
     const R b = omg * R(w7(q)) * th + R(w7(q)) * Ssrc;
     const R c4 = omg * R(4.0 * w7(q)) * th * cdot<R, cx, cy, cz>(ux, uy, uz);
-    __stcs(gB + (uint32_t)q * qs + n, K::enc_g((a * X.g[q] + b + c4) * one_sg));
-    __stcs(gB + (uint32_t)(q + 1) * qs + n, K::enc_g((a * X.g[q + 1] + b - c4) * one_sg));
+    K::store(gB + (n + D.plane[q]), K::enc_g((a * X.g[q] + b + c4) * one_sg));
+    K::store(gB + (n + D.plane[q + 1]), K::enc_g((a * X.g[q + 1] + b - c4) * one_sg));
   });
   M.rho = rho;
   M.jx = jx;
@@ -601,6 +596,7 @@ __device__ __forceinline__ void step_block(const DomainView& D, int bx, int by, 
     Column<R> C;
     load_column(D, P, i, j, C);
     const uint32_t base = (uint32_t)j * (uint32_t)D.px + (uint32_t)i;
+#pragma unroll 1
     for (int k = max(k0, C.kg); k < k1; ++k) {
       const uint32_t n = (uint32_t)k * D.ps + base;
       Cell<R> X;

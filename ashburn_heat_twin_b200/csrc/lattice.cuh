@@ -62,6 +62,7 @@ struct Codec<float> {
   using Real = float;
   static constexpr int kBytes = 4;
   __device__ __forceinline__ static float load(const float* p) { return __ldg(p); }
+  __device__ __forceinline__ static void store(float* p, float v) { __stcs(p, v); }
   __device__ __forceinline__ static float dec_f(float v, float /*w*/) { return v; }
   __device__ __forceinline__ static float dec_g(float v) { return v; }
   __device__ __forceinline__ static float enc_f(float v, float /*w*/) { return v; }
@@ -73,23 +74,33 @@ struct Codec<double> {
   using Real = double;
   static constexpr int kBytes = 8;
   __device__ __forceinline__ static double load(const double* p) { return __ldg(p); }
+  __device__ __forceinline__ static void store(double* p, double v) { __stcs(p, v); }
   __device__ __forceinline__ static double dec_f(double v, double /*w*/) { return v; }
   __device__ __forceinline__ static double dec_g(double v) { return v; }
   __device__ __forceinline__ static double enc_f(double v, double /*w*/) { return v; }
   __device__ __forceinline__ static double enc_g(double v) { return v; }
 };
 
+// The 16-bit codecs scale by powers of two, so (f - w)*s and h/s + w written as one FMA round exactly like the
+// separate multiply and add (the product is exact): the contraction changes no bits.
 template <>
 struct Codec<__half> {
   using Real = float;
   static constexpr int kBytes = 2;
-  __device__ __forceinline__ static __half load(const __half* p) { return __ldg(p); }
+  // 16-bit traffic goes through the unsigned short load / store builtins (the __half overloads are inline-asm
+  // wrappers the scheduler cannot reason about)
+  __device__ __forceinline__ static __half load(const __half* p) {
+    return __ushort_as_half(__ldg(reinterpret_cast<const unsigned short*>(p)));
+  }
+  __device__ __forceinline__ static void store(__half* p, __half v) {
+    __stcs(reinterpret_cast<unsigned short*>(p), __half_as_ushort(v));
+  }
   __device__ __forceinline__ static float dec_f(__half v, float w) {
-    return __fadd_rn(w, __fmul_rn(__half2float(v), 1.0f / kScaleF16));
+    return __fmaf_rn(__half2float(v), 1.0f / kScaleF16, w);
   }
   __device__ __forceinline__ static float dec_g(__half v) { return __fmul_rn(__half2float(v), 1.0f / kScaleG16); }
   __device__ __forceinline__ static __half enc_f(float v, float w) {
-    return __float2half_rn(__fmul_rn(__fsub_rn(v, w), kScaleF16));
+    return __float2half_rn(__fmaf_rn(v, kScaleF16, -kScaleF16 * w));
   }
   __device__ __forceinline__ static __half enc_g(float v) { return __float2half_rn(__fmul_rn(v, kScaleG16)); }
 };
@@ -98,15 +109,20 @@ template <>
 struct Codec<__nv_bfloat16> {
   using Real = float;
   static constexpr int kBytes = 2;
-  __device__ __forceinline__ static __nv_bfloat16 load(const __nv_bfloat16* p) { return __ldg(p); }
+  __device__ __forceinline__ static __nv_bfloat16 load(const __nv_bfloat16* p) {
+    return __ushort_as_bfloat16(__ldg(reinterpret_cast<const unsigned short*>(p)));
+  }
+  __device__ __forceinline__ static void store(__nv_bfloat16* p, __nv_bfloat16 v) {
+    __stcs(reinterpret_cast<unsigned short*>(p), __bfloat16_as_ushort(v));
+  }
   __device__ __forceinline__ static float dec_f(__nv_bfloat16 v, float w) {
-    return __fadd_rn(w, __fmul_rn(__bfloat162float(v), 1.0f / kScaleBF16));
+    return __fmaf_rn(__bfloat162float(v), 1.0f / kScaleBF16, w);
   }
   __device__ __forceinline__ static float dec_g(__nv_bfloat16 v) {
     return __fmul_rn(__bfloat162float(v), 1.0f / kScaleBF16);
   }
   __device__ __forceinline__ static __nv_bfloat16 enc_f(float v, float w) {
-    return __float2bfloat16_rn(__fmul_rn(__fsub_rn(v, w), kScaleBF16));
+    return __float2bfloat16_rn(__fmaf_rn(v, kScaleBF16, -kScaleBF16 * w));
   }
   __device__ __forceinline__ static __nv_bfloat16 enc_g(float v) {
     return __float2bfloat16_rn(__fmul_rn(v, kScaleBF16));
@@ -138,6 +154,20 @@ struct DomainView {
   int nx, ny, nz, px;
   uint32_t ps;                  // plane stride px*ny
   uint32_t qs;                  // q stride px*ny*nz
+  // element offset of the interior pull source of population q relative to the cell: q*qs - (cx + cy*px + cz*ps)
+  // (kernel-parameter table, so each gather is one add of a constant operand)
+  uint32_t pull_f[19], pull_g[7];
+  uint32_t plane[19];           // q*qs
 };
+
+// fill the offset tables of a view from its strides
+inline void set_offsets(DomainView& D) {   // host only
+  for (int q = 0; q < 19; ++q) {
+    D.plane[q] = (uint32_t)q * D.qs;
+    D.pull_f[q] = (uint32_t)q * D.qs - (uint32_t)(kC19[q][0] + kC19[q][1] * D.px + kC19[q][2] * (int)D.ps);
+  }
+  for (int q = 0; q < 7; ++q)
+    D.pull_g[q] = (uint32_t)q * D.qs - (uint32_t)(kC7[q][0] + kC7[q][1] * D.px + kC7[q][2] * (int)D.ps);
+}
 
 }  // namespace ahx

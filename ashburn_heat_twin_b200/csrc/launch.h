@@ -14,6 +14,7 @@ struct StepLaunch {
   bool budget;
   int block_y;     // threads per block in y (x is one warp)
   int zslab;       // levels per block
+  int minb = 0;    // 0, or 4 / 5 / 6 resident 128-thread blocks per SM (register budget 128 / 96 / 80)
 };
 
 // fused step, IEEE-exact arithmetic (step_exact.cu, built with -fmad=false)

@@ -13,19 +13,36 @@ namespace AHX_STEP_NS {
 #define AHX_STEP_FAST 0
 #endif
 
-template <class S, int MODE, bool BUDGET>
-__global__ void __launch_bounds__(256) step_kernel(DomainView D, int zslab) {
+// MINB = 0: up to 256 threads per block, registers as the compiler likes; MINB = 4 / 5 / 6: 128-thread blocks with
+// 4 / 5 / 6 resident per SM (a 128 / 96 / 80 register budget), chosen by the launch-shape tuner
+template <class S, int MODE, bool BUDGET, int MINB>
+__global__ void __launch_bounds__(MINB ? 128 : 256, MINB ? MINB : 1) step_kernel(DomainView D, int zslab) {
   step_block<S, MODE, BUDGET, AHX_STEP_FAST != 0>(D, blockIdx.x, blockIdx.y, blockIdx.z, zslab);
 }
 
 template <class S, int MODE, bool BUDGET>
 static cudaError_t launch_t(const DomainView& D, const StepLaunch& L, cudaStream_t s) {
-  const int by = L.block_y > 0 ? L.block_y : 4;
+  const int minb = (MODE == 0 && !BUDGET) ? L.minb : 0;
+  const int by = minb ? 4 : (L.block_y > 0 ? L.block_y : 4);
   const int zs = L.zslab > 0 ? L.zslab : D.nz;
   dim3 block(kBlockX, by);
   dim3 grid((D.nx + kBlockX - 1) / kBlockX, (D.ny + by - 1) / by, (D.nz + zs - 1) / zs);
   const size_t smem = (size_t)D.nz * sizeof(float4);
-  step_kernel<S, MODE, BUDGET><<<grid, block, smem, s>>>(D, zs);
+  if constexpr (MODE == 0 && !BUDGET) {
+    if (minb == 4) {
+      step_kernel<S, MODE, BUDGET, 4><<<grid, block, smem, s>>>(D, zs);
+      return cudaGetLastError();
+    }
+    if (minb == 5) {
+      step_kernel<S, MODE, BUDGET, 5><<<grid, block, smem, s>>>(D, zs);
+      return cudaGetLastError();
+    }
+    if (minb == 6) {
+      step_kernel<S, MODE, BUDGET, 6><<<grid, block, smem, s>>>(D, zs);
+      return cudaGetLastError();
+    }
+  }
+  step_kernel<S, MODE, BUDGET, 0><<<grid, block, smem, s>>>(D, zs);
   return cudaGetLastError();
 }
 

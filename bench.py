@@ -179,6 +179,8 @@ def main():
     ap.add_argument('--frame', type=int, default=10, help='steps per e2e frame (setMet + step(F) + read())')
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--no-autotune', action='store_true')
+    ap.add_argument('--block-y', type=int, default=0, help='fix the launch shape instead of autotuning')
+    ap.add_argument('--zslab', type=int, default=0)
     ap.add_argument('--workload', default='c2', choices=sorted(WORKLOADS),
                     help='c2 (the benchmark) or c1 (a smaller case for profiling)')
     a = ap.parse_args()
@@ -207,7 +209,10 @@ def main():
     cells = nx * ny * nz
     fluid = s.info['nFluid']
     tune = None
-    if not a.no_autotune:
+    if a.block_y or a.zslab:
+        dev.set_launch(a.block_y, a.zslab)
+        tune = (a.block_y, a.zslab, None)
+    elif not a.no_autotune:
         tune = dev.autotune(3)
         log(f'[rank {rank}] autotune: block_y {tune[0]} zslab {tune[1]} {tune[2]:.3f} ms/step')
     dev.time_steps(a.warmup)

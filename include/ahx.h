@@ -178,9 +178,12 @@ ahx_status ahx_budget_read(ahx_handle* h, ahx_budget_out* out, int reset);
 
 /* --- tuning ----------------------------------------------------------------------------------------------------- */
 
-/* launch shape of the fused step: threads per block in y (x is one warp), z-slab depth in levels; 0 = keep */
+/* launch shape of the fused step: block_y = threads per block in y (x is one warp) plus 100 x the register-budget
+ * variant (0: compiler's choice; 4, 5 or 6: 128-thread blocks, that many resident per SM, only with block_y 4), z-slab
+ * depth in levels; 0 = keep */
 ahx_status ahx_set_launch(ahx_handle* h, int block_y, int zslab);
-/* time candidate launch shapes on scratch copies of the state and keep the fastest; the state is not advanced */
+/* time candidate launch shapes on scratch copies of the state and keep the fastest; the state is not advanced;
+ * *best_block_y uses the encoding of ahx_set_launch */
 ahx_status ahx_autotune(ahx_handle* h, int steps_per_trial, int* best_block_y, int* best_zslab, float* best_ms);
 
 #ifdef __cplusplus
