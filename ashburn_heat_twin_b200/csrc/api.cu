@@ -60,6 +60,8 @@ struct Fence {
 
 }  // namespace
 
+void ahx::set_last_error(const std::string& m) { g_err = m; }
+
 struct ahx_handle {
   std::mutex mu;
   int dev = 0;
@@ -838,7 +840,7 @@ ahx_status ahx_autotune(ahx_handle* h, int steps_per_trial, int* best_block_y, i
   h->block_y = bby;
   h->zslab = bzs;
   h->minb = bmb;
-  if (best_block_y) *best_block_y = bby * 100 + bmb;   // block_y, and the register-budget variant in the hundreds
+  if (best_block_y) *best_block_y = bmb * 100 + bby;   // the ahx_set_launch encoding: variant x 100 + block_y
   if (best_zslab) *best_zslab = bzs;
   if (best_ms) *best_ms = best;
   return AHX_OK;

@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <string>
+
 #include "lattice.cuh"
 
 namespace ahx {
@@ -51,5 +53,8 @@ cudaError_t launch_export_plane(const DomainView& D, int precision, const void* 
                                 int q, int is_g, cudaStream_t s);
 
 int element_bytes(int precision);
+
+// the thread-local message ahx_last_error() returns (api.cu)
+void set_last_error(const std::string& m);
 
 }  // namespace ahx
