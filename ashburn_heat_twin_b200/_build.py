@@ -34,6 +34,7 @@ UNITS = {
     'step_fast.cu': ['-fmad=true', '-prec-div=false', '-prec-sqrt=false'],
     'aux.cu': ['-fmad=false'] + IEEE,
     'api.cu': ['-fmad=false'] + IEEE,
+    'noalloc.cu': ['-fmad=false'] + IEEE,
 }
 
 

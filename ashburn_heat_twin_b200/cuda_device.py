@@ -24,7 +24,7 @@ SYMBOLS = ('ahx_create', 'ahx_destroy', 'ahx_last_error', 'ahx_get_info', 'ahx_s
            'ahx_set_ktop', 'ahx_init_flow', 'ahx_clear_heat', 'ahx_set_parity', 'ahx_step', 'ahx_sync', 'ahx_fence',
            'ahx_fence_query', 'ahx_read_submit', 'ahx_read_wait', 'ahx_read_state', 'ahx_write_state',
            'ahx_read_state_f64', 'ahx_write_state_f64', 'ahx_read_dbg', 'ahx_clear_dbg', 'ahx_stats',
-           'ahx_budget_enable', 'ahx_budget_read', 'ahx_set_launch', 'ahx_autotune', 'ahx_time_steps')
+           'ahx_budget_enable', 'ahx_budget_read', 'ahx_set_launch', 'ahx_autotune', 'ahx_time_steps', 'ahx_stats_noalloc')
 
 
 class AhxError(RuntimeError):
@@ -99,6 +99,7 @@ def load_library(path: str = LIB_PATH):
         'ahx_set_launch': [H, i, i],
         'ahx_autotune': [H, i, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
                          ctypes.POINTER(ctypes.c_float)],
+        'ahx_stats_noalloc': [i, i, i, vp, vp, vp, vp, vp],
     }
     for name, args in sig.items():
         fn = getattr(L, name)
