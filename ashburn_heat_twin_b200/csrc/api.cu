@@ -5,6 +5,7 @@
 // reference's single WebGPU queue, solver.js:401-427). Read-back runs its two small kernels on that stream and copies
 // on a second stream, so a read never stalls stepping (solver.js:439-471). Host images are staged through a ring of
 // pinned buffers so an upload between steps does not wait for the GPU (the reference's queue.writeBuffer).
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <chrono>
@@ -85,6 +86,10 @@ struct ahx_handle {
   int parity = 0;
   int64_t steps = 0;
   int block_y = 4, zslab = 0, minb = 0;
+  int tma_ty = 0, tma_depth = 0;          // staged kernel selected when tma_ty > 0
+  bool maps_ok = false;
+  TmaMaps maps[2][2];                     // [TY 4 / 8][parity]: tensor maps of the state read by a step
+  int* d_err = nullptr;                   // error word the staged kernel sets
   ReadSlot reads[AHX_MAX_READS];
   uint64_t next_read = 0;
   UploadSlot up[kUploadSlots];
@@ -134,6 +139,7 @@ DomainView view(ahx_handle* h) {
   D.gB = h->g[1 - h->parity];
   D.dbg = h->d_dbg;
   D.budget = h->d_budget;
+  D.err = h->d_err;
   D.nx = h->dims.nx;
   D.ny = h->dims.ny;
   D.nz = h->dims.nz;
@@ -142,6 +148,60 @@ DomainView view(ahx_handle* h) {
   D.qs = h->qs;
   set_offsets(D);
   return D;
+}
+
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+    cudaGetLastError();
+  });
+  return fn;
+}
+
+// 4-D tensor map [q][z][y][x] over one population buffer with a box of width x TY x 1 x 1
+bool encode_map(ahx_handle* h, void* buf, int nq, int width, int ty, CUtensorMap* out) {
+  EncodeTiledFn fn = encode_fn();
+  if (!fn) return false;
+  const int es = h->esize;
+  const CUtensorMapDataType dt = es == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
+                                 : es == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64
+                                           : CU_TENSOR_MAP_DATA_TYPE_UINT16;
+  const cuuint64_t dims[4] = {(cuuint64_t)h->dims.nx, (cuuint64_t)h->dims.ny, (cuuint64_t)h->dims.nz, (cuuint64_t)nq};
+  const cuuint64_t strides[3] = {(cuuint64_t)h->px * es, (cuuint64_t)h->ps * es, (cuuint64_t)h->qs * es};
+  const cuuint32_t box[4] = {(cuuint32_t)width, (cuuint32_t)ty, 1, 1};
+  const cuuint32_t estr[4] = {1, 1, 1, 1};
+  return fn(out, dt, 4, buf, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// the four maps (f wide / narrow, g wide / narrow) of a state (f, g) for blocks of 32 x ty columns
+bool make_maps(ahx_handle* h, void* f, void* g, int ty, TmaMaps* M) {
+  const int H = 16 / h->esize;
+  return encode_map(h, f, 19, 32 + 2 * H, ty, &M->fw) && encode_map(h, f, 19, 32, ty, &M->fn) &&
+         encode_map(h, g, 7, 32 + 2 * H, ty, &M->gw) && encode_map(h, g, 7, 32, ty, &M->gn);
+}
+
+// a staged copy that ran out of time leaves its block's cells unstepped: report it (the state is not usable)
+ahx_status check_kernel_error(ahx_handle* h) {
+  int e = 0;
+  if (cudaMemcpy(&e, h->d_err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+    return cuda_fail(h, cudaGetLastError(), "error word read");
+  if (e != 0) {
+    h->lost = true;
+    h->lost_msg = "a TMA stage of the step kernel did not arrive within its time bound";
+    return fail(AHX_ETIMEOUT, "live solver: " + h->lost_msg);
+  }
+  return AHX_OK;
 }
 
 // copy a host image to device memory in stream order without blocking the host on the GPU
@@ -184,7 +244,7 @@ void free_all(ahx_handle* h) {
     if (h->g[p]) cudaFree(h->g[p]);
     h->f[p] = h->g[p] = nullptr;
   }
-  void* devs[] = {h->d_params, h->d_colv, h->d_ktop, h->d_oldk, h->d_dbg, h->d_budget, h->d_stats};
+  void* devs[] = {h->d_params, h->d_colv, h->d_ktop, h->d_oldk, h->d_dbg, h->d_budget, h->d_stats, h->d_err};
   for (void* p : devs)
     if (p) cudaFree(p);
   h->d_params = nullptr;
@@ -193,6 +253,7 @@ void free_all(ahx_handle* h) {
   h->d_dbg = nullptr;
   h->d_budget = nullptr;
   h->d_stats = nullptr;
+  h->d_err = nullptr;
   for (auto& r : h->reads) {
     if (r.d_surf) cudaFree(r.d_surf);
     if (r.d_vol) cudaFree(r.d_vol);
@@ -299,8 +360,13 @@ ahx_status ahx_create(const ahx_dims* dims, ahx_handle** out) {
       cudaMalloc(&h->d_colv, NXY * sizeof(uint4)) != cudaSuccess ||
       cudaMalloc(&h->d_ktop, NXY * 4) != cudaSuccess || cudaMalloc(&h->d_oldk, NXY * 4) != cudaSuccess ||
       cudaMalloc(&h->d_budget, (size_t)kBudgetSlots * kBudgetStride * sizeof(double)) != cudaSuccess ||
-      cudaMalloc(&h->d_stats, sizeof(StatsScratch)) != cudaSuccess)
+      cudaMalloc(&h->d_stats, sizeof(StatsScratch)) != cudaSuccess ||
+      cudaMalloc(&h->d_err, sizeof(int)) != cudaSuccess)
     return bail(AHX_ENOMEM, "live solver: buffer allocation failed (out of memory)");
+  cudaMemsetAsync(h->d_err, 0, sizeof(int), h->s_step);
+  h->maps_ok = true;
+  for (int t = 0; t < 2; ++t)
+    for (int p = 0; p < 2; ++p) h->maps_ok = h->maps_ok && make_maps(h, h->f[p], h->g[p], t ? 8 : 4, &h->maps[t][p]);
   cudaMemsetAsync(h->d_params, 0, 64 + 16 * (size_t)dims->nz, h->s_step);
   cudaMemsetAsync(h->d_colv, 0, NXY * sizeof(uint4), h->s_step);
   cudaMemsetAsync(h->d_ktop, 0, NXY * 4, h->s_step);
@@ -436,8 +502,11 @@ ahx_status ahx_step(ahx_handle* h, int n, int mode) {
   L.block_y = h->block_y;
   L.zslab = h->zslab;
   L.minb = h->minb;
+  L.tma_ty = h->maps_ok ? h->tma_ty : 0;
+  L.tma_depth = h->tma_depth;
   for (int s = 0; s < n; ++s) {
     L.mode = (mode == AHX_MODE_ACC) ? 2 : ((mode == AHX_MODE_OUT && s == n - 1) ? 1 : 0);
+    L.maps = L.tma_ty ? &h->maps[L.tma_ty == 8 ? 1 : 0][h->parity] : nullptr;
     DomainView D = view(h);
     const cudaError_t e = h->dims.arith == AHX_ARITH_FAST ? fast::launch_step(D, L, h->s_step)
                                                             : exact::launch_step(D, L, h->s_step);
@@ -472,6 +541,10 @@ ahx_status ahx_time_steps(ahx_handle* h, int n, int mode, int timeout_ms, float*
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  if (st == AHX_OK) {
+    std::lock_guard<std::mutex> lk(h->mu);
+    st = check_kernel_error(h);
+  }
   return st;
 }
 
@@ -485,8 +558,12 @@ ahx_status ahx_sync(ahx_handle* h, int timeout_ms) {
     AHX_CUDA(h, cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
     AHX_CUDA(h, cudaEventRecord(ev, h->s_step));
   }
-  const ahx_status st = wait_event(h, ev, timeout_ms);
+  ahx_status st = wait_event(h, ev, timeout_ms);
   cudaEventDestroy(ev);
+  if (st == AHX_OK) {
+    std::lock_guard<std::mutex> lk(h->mu);
+    st = check_kernel_error(h);
+  }
   return st;
 }
 
@@ -746,12 +823,25 @@ ahx_status ahx_set_launch(ahx_handle* h, int block_y, int zslab) {
   if (!h) return fail(AHX_EINVAL, "live solver: null handle");
   std::lock_guard<std::mutex> lk(h->mu);
   if (ahx_status st = check(h)) return st;
-  const int by = block_y % 100, mb = block_y / 100;
-  if (by < 0 || by > 8 || zslab < 0 || (mb != 0 && (mb < 4 || mb > 6)) || (mb && by != 4))
-    return fail(AHX_EINVAL, "live solver: bad launch shape");
-  if (block_y) {
-    h->block_y = by;
-    h->minb = mb;
+  if (block_y >= 1000) {   // staged kernel: 1000 + 100 x depth + rows (4 with depth 2-4, or 8 with depth 2-3)
+    const int ty = block_y % 100, dp = (block_y / 100) % 10;
+    if (!((ty == 4 && dp >= 2 && dp <= 4) || (ty == 8 && dp >= 2 && dp <= 3)) || zslab < 0)
+      return fail(AHX_EINVAL, "live solver: bad staged launch shape");
+    if (!h->maps_ok) return fail(AHX_EINVAL, "live solver: tensor maps unavailable for the staged kernel");
+    h->tma_ty = ty;
+    h->tma_depth = dp;
+    h->block_y = ty;
+    h->minb = 0;
+  } else {
+    const int by = block_y % 100, mb = block_y / 100;
+    if (by < 0 || by > 8 || zslab < 0 || (mb != 0 && (mb < 4 || mb > 6)) || (mb && by != 4))
+      return fail(AHX_EINVAL, "live solver: bad launch shape");
+    if (block_y) {
+      h->block_y = by;
+      h->minb = mb;
+      h->tma_ty = 0;
+      h->tma_depth = 0;
+    }
   }
   if (zslab) h->zslab = zslab;
   return AHX_OK;
@@ -781,12 +871,21 @@ ahx_status ahx_autotune(ahx_handle* h, int steps_per_trial, int* best_block_y, i
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
   struct Shape {
-    int by, minb;
+    int by, minb, ty, depth;
   };
-  const Shape shapes[] = {{2, 0}, {4, 0}, {8, 0}, {4, 4}, {4, 5}, {4, 6}};
+  std::vector<Shape> shapes = {{2, 0, 0, 0}, {4, 0, 0, 0}, {8, 0, 0, 0}, {4, 4, 0, 0}, {4, 5, 0, 0}, {4, 6, 0, 0}};
+  // staged (TMA) shapes, with tensor maps over the scratch copies the trials step
+  TmaMaps tm[2][2];
+  bool tma_ok = h->maps_ok;
+  for (int t = 0; t < 2 && tma_ok; ++t) {
+    tma_ok = make_maps(h, f0, g0, t ? 8 : 4, &tm[t][0]) && make_maps(h, f1, g1, t ? 8 : 4, &tm[t][1]);
+  }
+  if (tma_ok)
+    for (Shape sh : {Shape{4, 0, 4, 2}, Shape{4, 0, 4, 3}, Shape{4, 0, 4, 4}, Shape{8, 0, 8, 2}, Shape{8, 0, 8, 3}})
+      shapes.push_back(sh);
   std::vector<int> zss = {h->dims.nz, 32, 16, 8};
   float best = 1e30f;
-  int bby = h->block_y, bzs = h->zslab, bmb = h->minb;
+  int bby = h->block_y, bzs = h->zslab, bmb = h->minb, bty = h->tma_ty, bdp = h->tma_depth;
   DomainView D = view(h);
   D.dbg = nullptr;
   StepLaunch L;
@@ -797,8 +896,11 @@ ahx_status ahx_autotune(ahx_handle* h, int steps_per_trial, int* best_block_y, i
   for (const Shape& sh : shapes) {
     for (int zs : zss) {
       if (zs > h->dims.nz) continue;
+      if (sh.ty && zs < 16) continue;   // the staged kernel needs a few levels per block to fill its pipeline
       L.block_y = sh.by;
       L.minb = sh.minb;
+      L.tma_ty = sh.ty;
+      L.tma_depth = sh.depth;
       L.zslab = zs;
       float ms = 0;
       for (int rep = 0; rep < 2 && st == AHX_OK; ++rep) {   // rep 0 warms up
@@ -808,6 +910,7 @@ ahx_status ahx_autotune(ahx_handle* h, int steps_per_trial, int* best_block_y, i
           D.fB = (s & 1) ? f0 : f1;
           D.gA = (s & 1) ? g1 : g0;
           D.gB = (s & 1) ? g0 : g1;
+          L.maps = sh.ty ? &tm[sh.ty == 8 ? 1 : 0][s & 1] : nullptr;
           const cudaError_t e = h->dims.arith == AHX_ARITH_FAST ? fast::launch_step(D, L, h->s_step)
                                                                   : exact::launch_step(D, L, h->s_step);
           if (e != cudaSuccess) {
@@ -826,9 +929,12 @@ ahx_status ahx_autotune(ahx_handle* h, int steps_per_trial, int* best_block_y, i
         bby = sh.by;
         bzs = zs;
         bmb = sh.minb;
+        bty = sh.ty;
+        bdp = sh.depth;
       }
     }
   }
+  if (st == AHX_OK) st = check_kernel_error(h);
   cudaStreamSynchronize(h->s_step);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
@@ -840,7 +946,10 @@ ahx_status ahx_autotune(ahx_handle* h, int steps_per_trial, int* best_block_y, i
   h->block_y = bby;
   h->zslab = bzs;
   h->minb = bmb;
-  if (best_block_y) *best_block_y = bmb * 100 + bby;   // the ahx_set_launch encoding: variant x 100 + block_y
+  h->tma_ty = bty;
+  h->tma_depth = bdp;
+  // the ahx_set_launch encoding: variant x 100 + block_y, or 1000 + 100 x depth + rows for the staged kernel
+  if (best_block_y) *best_block_y = bty ? 1000 + 100 * bdp + bty : bmb * 100 + bby;
   if (best_zslab) *best_zslab = bzs;
   if (best_ms) *best_ms = best;
   return AHX_OK;

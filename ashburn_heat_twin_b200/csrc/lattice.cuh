@@ -151,6 +151,7 @@ struct DomainView {
   void* gB;
   float4* dbg;                  // (theta, ux, uy, uz) per cell (pitched), or null
   double* budget;               // per-step FP64 budget accumulators, or null
+  int* err;                     // error word: a staged copy that did not arrive in time sets it
   int nx, ny, nz, px;
   uint32_t ps;                  // plane stride px*ny
   uint32_t qs;                  // q stride px*ny*nz

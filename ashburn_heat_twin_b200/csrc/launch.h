@@ -7,6 +7,7 @@
 #include <string>
 
 #include "lattice.cuh"
+#include "tma.cuh"
 
 namespace ahx {
 
@@ -17,6 +18,9 @@ struct StepLaunch {
   int block_y;     // threads per block in y (x is one warp)
   int zslab;       // levels per block
   int minb = 0;    // 0, or 4 / 5 / 6 resident 128-thread blocks per SM (register budget 128 / 96 / 80)
+  int tma_ty = 0;  // > 0: the TMA-staged kernel with 32 x tma_ty columns per block ...
+  int tma_depth = 0;               // ... and this many levels staged ahead
+  const TmaMaps* maps = nullptr;   // tensor maps of the state being read
 };
 
 // fused step, IEEE-exact arithmetic (step_exact.cu, built with -fmad=false)

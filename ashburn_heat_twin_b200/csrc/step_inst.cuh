@@ -5,6 +5,7 @@
 
 #include "fused.cuh"
 #include "launch.h"
+#include "tma.cuh"
 
 namespace ahx {
 namespace AHX_STEP_NS {
@@ -20,8 +21,50 @@ __global__ void __launch_bounds__(MINB ? 128 : 256, MINB ? MINB : 1) step_kernel
   step_block<S, MODE, BUDGET, AHX_STEP_FAST != 0>(D, blockIdx.x, blockIdx.y, blockIdx.z, zslab);
 }
 
+template <class S, int TY, int DEPTH>
+__global__ void __launch_bounds__(32 * TY, TY == 4 ? 4 : 2)
+    step_tma_kernel(DomainView D, const __grid_constant__ TmaMaps M, int zslab) {
+  step_tma_block<S, AHX_STEP_FAST != 0, TY, DEPTH>(D, M, zslab);
+}
+
+template <class S, int TY, int DEPTH>
+static cudaError_t launch_tma_t(const DomainView& D, const StepLaunch& L, cudaStream_t s) {
+  const int zs = L.zslab > 0 ? L.zslab : D.nz;
+  const size_t smem = tma_smem_bytes<S, TY, DEPTH>(D.nz);
+  // the dynamic shared-memory size the attribute allows, per device (an attribute is per function and device)
+  static int configured[64] = {0};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64 || configured[dev] < (int)smem) {
+    const cudaError_t e = cudaFuncSetAttribute(step_tma_kernel<S, TY, DEPTH>,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    if (dev >= 0 && dev < 64) configured[dev] = (int)smem;
+  }
+  dim3 block(32, TY);
+  dim3 grid((D.nx + 31) / 32, (D.ny + TY - 1) / TY, (D.nz + zs - 1) / zs);
+  step_tma_kernel<S, TY, DEPTH><<<grid, block, smem, s>>>(D, *L.maps, zs);
+  return cudaGetLastError();
+}
+
+template <class S>
+static cudaError_t launch_tma(const DomainView& D, const StepLaunch& L, cudaStream_t s) {
+  const int key = L.tma_ty * 10 + L.tma_depth;
+  switch (key) {
+    case 42: return launch_tma_t<S, 4, 2>(D, L, s);
+    case 43: return launch_tma_t<S, 4, 3>(D, L, s);
+    case 44: return launch_tma_t<S, 4, 4>(D, L, s);
+    case 82: return launch_tma_t<S, 8, 2>(D, L, s);
+    case 83: return launch_tma_t<S, 8, 3>(D, L, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
 template <class S, int MODE, bool BUDGET>
 static cudaError_t launch_t(const DomainView& D, const StepLaunch& L, cudaStream_t s) {
+  if constexpr (MODE == 0 && !BUDGET) {
+    if (L.tma_ty > 0 && L.maps != nullptr) return launch_tma<S>(D, L, s);
+  }
   const int minb = (MODE == 0 && !BUDGET) ? L.minb : 0;
   const int by = minb ? 4 : (L.block_y > 0 ? L.block_y : 4);
   const int zs = L.zslab > 0 ? L.zslab : D.nz;

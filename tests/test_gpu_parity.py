@@ -194,3 +194,19 @@ def test_autotune_keeps_state():
     assert _state_equal(g, o)
     g.destroy()
     o.destroy()
+
+
+@pytest.mark.parametrize('shape', [1204, 1304, 1404, 1208, 1308, 504, 404])
+@pytest.mark.parametrize('zslab', [0, 12])
+def test_launch_shapes_bit_exact(shape, zslab):
+    """Every launch shape of the exact build (TMA-staged kernel: 1000 + 100 x stages + rows; register-budget
+    variants 404 / 504), with whole columns or 12-level z-slabs, stays bit-identical to the oracle."""
+    met = dict(u10=5.0, dirFrom=300.0, wstar=1.5, blh=700.0)
+    g, o = _pair(met=met)
+    g._dev.set_launch(shape, zslab)
+    for s in (g, o):
+        s._dbg.stepOut(6).result()
+    assert _state_equal(g, o)
+    assert np.array_equal(g._dbg.readDbg(), o._dbg.readDbg())
+    g.destroy()
+    o.destroy()
