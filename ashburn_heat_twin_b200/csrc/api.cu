@@ -917,6 +917,15 @@ ahx_status ahx_autotune(ahx_handle* h, int steps_per_trial, int* best_block_y, i
             st = cuda_fail(h, e, "autotune launch");
             break;
           }
+          // each trial launch completes before the next is queued, so an error is charged to the shape that made it
+          const cudaError_t e2 = cudaStreamSynchronize(h->s_step);
+          if (e2 != cudaSuccess) {
+            char what[96];
+            std::snprintf(what, sizeof(what), "autotune trial (rows %d, variant %d, staged %d/%d, zslab %d)", sh.by,
+                          sh.minb, sh.ty, sh.depth, zs);
+            st = cuda_fail(h, e2, what);
+            break;
+          }
         }
         cudaEventRecord(e1, h->s_step);
         cudaEventSynchronize(e1);

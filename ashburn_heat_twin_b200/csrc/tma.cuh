@@ -85,8 +85,15 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity
   return true;
 }
 
+// One box copy. The tensor map (64 B), destination (128 B) and barrier (8 B) alignments the copy engine requires are
+// checked first: a violation sets the error word and skips the copy (its stage then never completes and the block
+// aborts through its bounded wait) instead of faulting.
 __device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, int x, int y, int z, int w,
-                                            uint64_t* bar) {
+                                            uint64_t* bar, int* err) {
+  if (((reinterpret_cast<uint64_t>(map) & 63) | (smem_u32(dst) & 127) | (smem_u32(bar) & 7)) != 0) {
+    atomicExch(err, 2);
+    return;
+  }
   asm volatile(
       "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
       "[%6];" ::"r"(smem_u32(dst)),
@@ -98,22 +105,22 @@ constexpr uint64_t kStageWaitLimitNs = 200ull * 1000 * 1000;   // 200 ms: far be
 
 template <class S, int TY>
 __device__ __forceinline__ void tma_issue_level(const TmaMaps& M, unsigned char* stage, uint64_t* bar, int x0,
-                                                int j0, int k) {
+                                                int j0, int k, int* err) {
   using G = TmaGeom<S>;
   mbar_arm(bar, (unsigned)G::template stage_bytes<TY>());
   static_for<19>([&](auto Q) {
     constexpr int q = Q;
     constexpr int cx = kC19[q][0], cy = kC19[q][1], cz = kC19[q][2];
     constexpr int off = G::template box_offset<TY>(q);
-    if constexpr (cx != 0) tma_load_4d(stage + off, &M.fw, x0 - G::H, j0 - cy, k - cz, q, bar);
-    else tma_load_4d(stage + off, &M.fn, x0, j0 - cy, k - cz, q, bar);
+    if constexpr (cx != 0) tma_load_4d(stage + off, &M.fw, x0 - G::H, j0 - cy, k - cz, q, bar, err);
+    else tma_load_4d(stage + off, &M.fn, x0, j0 - cy, k - cz, q, bar, err);
   });
   static_for<7>([&](auto Q) {
     constexpr int q = Q;
     constexpr int cx = kC7[q][0], cy = kC7[q][1], cz = kC7[q][2];
     constexpr int off = G::template box_offset<TY>(19 + q);
-    if constexpr (cx != 0) tma_load_4d(stage + off, &M.gw, x0 - G::H, j0 - cy, k - cz, q, bar);
-    else tma_load_4d(stage + off, &M.gn, x0, j0 - cy, k - cz, q, bar);
+    if constexpr (cx != 0) tma_load_4d(stage + off, &M.gw, x0 - G::H, j0 - cy, k - cz, q, bar, err);
+    else tma_load_4d(stage + off, &M.gn, x0, j0 - cy, k - cz, q, bar, err);
   });
 }
 
@@ -193,14 +200,16 @@ __device__ __forceinline__ void step_tma_block(const DomainView& D, const TmaMap
   const int kb = s_kmin;   // first level with a fluid cell in this block's slab
   if (tid == 0)
     for (int d = 0; d < DEPTH && kb + d < k1; ++d)
-      tma_issue_level<S, TY>(M, base + (size_t)d * STAGE, &bars[d], x0, j0, kb + d);
+      tma_issue_level<S, TY>(M, base + (size_t)d * STAGE, &bars[d], x0, j0, kb + d, D.err);
   const uint32_t cbase = (uint32_t)j * (uint32_t)D.px + (uint32_t)i;
   int it = 0;
   for (int k = kb; k < k1; ++k, ++it) {
     const int s = it % DEPTH;
     const unsigned parity = (unsigned)((it / DEPTH) & 1);
     unsigned char* stage = base + (size_t)s * STAGE;
-    if (!mbar_wait_bounded(&bars[s], parity, kStageWaitLimitNs)) s_abort = 1;
+    // a set error word (from this or another block) stops the step early instead of waiting on stages
+    if (*reinterpret_cast<volatile int*>(D.err) != 0) s_abort = 1;
+    else if (!mbar_wait_bounded(&bars[s], parity, kStageWaitLimitNs)) s_abort = 1;
     if (active && k >= C.kg && !s_abort) {
       const uint32_t n = (uint32_t)k * D.ps + cbase;
       Cell<R> X;
@@ -236,7 +245,15 @@ __device__ __forceinline__ void step_tma_block(const DomainView& D, const TmaMap
       }
       break;
     }
-    if (tid == 0 && k + DEPTH < k1) tma_issue_level<S, TY>(M, stage, &bars[s], x0, j0, k + DEPTH);
+    if (tid == 0 && k + DEPTH < k1) tma_issue_level<S, TY>(M, stage, &bars[s], x0, j0, k + DEPTH, D.err);
+  }
+  if (tid == 0 && !s_abort) {
+    // before the block exits, every stage it armed must have completed its last phase (bounded wait)
+    for (int st = 0; st < DEPTH; ++st) {
+      const int uses = (k1 - kb > st) ? ((k1 - kb - st + DEPTH - 1) / DEPTH) : 0;
+      if (uses > 0 && !mbar_wait_bounded(&bars[st], (unsigned)((uses - 1) & 1), kStageWaitLimitNs))
+        atomicExch(D.err, 1);
+    }
   }
 }
 
