@@ -37,6 +37,9 @@ C1 = SynthSpec(hills=8, relief_m=30.0, buildings=1500, side_m=(20.0, 120.0), hei
                seed=1)
 C2 = SynthSpec(hills=24, relief_m=40.0, buildings=4000, side_m=(15.0, 150.0), height_m=(8.0, 40.0), dc_count=211,
                dc_side_m=(60.0, 200.0), dc_height_m=(14.0, 25.0), seed=2)
+# a quarter of the 600x600 box with the same densities (300x300x64 at 10 m): profiling-sized, state still >> L2
+C2Q = SynthSpec(ncols=300, nrows=300, hills=6, relief_m=40.0, buildings=1000, side_m=(15.0, 150.0),
+                height_m=(8.0, 40.0), dc_count=53, dc_side_m=(60.0, 200.0), dc_height_m=(14.0, 25.0), seed=3)
 
 
 def _place(rng, n, side, box_w, box_h, occ, sub, allow_overlap_after=20):

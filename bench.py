@@ -34,6 +34,8 @@ WORKLOADS = {
                     '211 DC roofs', dx=10, heightM=640, met='C2_MET', spec='C2'),
     'c1': dict(desc='200x200x32 cells at 30 m (1.28 M), synthetic seed 1: 8 hills 0-30 m, 1500 buildings, '
                     '60 DC roofs', dx=30, heightM=960, met='C1_MET', spec='C1'),
+    'c2q': dict(desc='300x300x64 cells at 10 m (5.76 M), synthetic seed 3: 6 hills 0-40 m, 1000 buildings, '
+                     '53 DC roofs', dx=10, heightM=640, met='C2_MET', spec='C2Q'),
 }
 METRIC = 'GLUPS (all cells) of the fused D3Q19+D3Q7 step, 600x600x64'
 
@@ -175,7 +177,7 @@ def main():
     ap.add_argument('--warmup', type=int, default=5)
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
     ap.add_argument('--precision', default='fp32', choices=['fp32', 'fp16', 'bf16', 'fp64'])
-    ap.add_argument('--arith', default='exact', choices=['exact', 'fast'])
+    ap.add_argument('--arith', default='fast', choices=['exact', 'fast'])
     ap.add_argument('--frame', type=int, default=10, help='steps per e2e frame (setMet + step(F) + read())')
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--no-autotune', action='store_true')
@@ -283,7 +285,7 @@ def main():
         s_steps = s._steps
         cpu = cpu_baseline()
         del s_steps
-    metric = METRIC if a.workload == 'c2' else METRIC.replace('600x600x64', '200x200x32')
+    metric = METRIC.replace('600x600x64', WORKLOADS[a.workload]['desc'].split(' cells')[0])
     out = dict(metric=metric, value=value, unit='GLUPS', n_gpus=world, steps=a.steps, warmup=a.warmup,
                ms_per_step=ms_all / a.steps, higher_is_better=True, scaling='weak', vs_baseline=None,
                dtype={'fp32': 'f32', 'fp16': 'f16-store/f32', 'bf16': 'bf16-store/f32', 'fp64': 'f64'}[a.precision],
