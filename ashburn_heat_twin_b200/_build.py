@@ -7,6 +7,8 @@ Translation units and their arithmetic flags:
                               the paired collision
   aux.cu         -fmad=false  read-back, init, re-init, stats, layout conversion
   api.cu                      the C ABI (include/ahx.h)
+  batch.cu                    batched stepping (ahx_batch_*: tile tables, CUDA graph, stream ordering)
+  noalloc.cu                  diagnostics over caller-owned buffers without allocation
 All use -ftz=true (f32 subnormals flushed, as the CPU restatement does); all but step_fast.cu use IEEE division and
 square root.
 """
@@ -35,6 +37,7 @@ UNITS = {
     'aux.cu': ['-fmad=false'] + IEEE,
     'api.cu': ['-fmad=false'] + IEEE,
     'noalloc.cu': ['-fmad=false'] + IEEE,
+    'batch.cu': ['-fmad=false'] + IEEE,
 }
 
 

@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "ahx.h"
+#include "handle.h"
 #include "launch.h"
 
 using namespace ahx;
@@ -25,84 +26,17 @@ namespace {
 
 thread_local std::string g_err;
 
-ahx_status fail(ahx_status st, const std::string& msg) {
+}  // namespace
+
+ahx_status ahx::fail(ahx_status st, const std::string& msg) {
   g_err = msg;
   return st;
 }
 
-constexpr int kUploadSlots = 4;
-// column levels (kt, ktop) are validated against this bound so every level index stays a small non-negative int
-constexpr uint32_t kMaxLevel = 65535;
-
-struct ReadSlot {
-  bool busy = false;
-  uint64_t ticket = 0;
-  int nzv = 0, want_vol = 0, want_wind = 0;
-  float* d_surf = nullptr;     // 3*NXY
-  uint32_t* d_vol = nullptr;   // ceil(nz*NXY/4)
-  unsigned* d_tmax = nullptr;
-  float* h_surf = nullptr;     // pinned
-  uint8_t* h_vol = nullptr;    // pinned
-  unsigned* h_tmax = nullptr;  // pinned
-  cudaEvent_t ev_kernels = nullptr, ev_done = nullptr;
-};
-
-struct UploadSlot {
-  void* h = nullptr;   // pinned
-  size_t bytes = 0;
-  cudaEvent_t ev = nullptr;
-  bool used = false;
-};
-
-struct Fence {
-  uint64_t ticket;
-  cudaEvent_t ev;
-};
-
-}  // namespace
-
 void ahx::set_last_error(const std::string& m) { g_err = m; }
 
-struct ahx_handle {
-  std::mutex mu;
-  int dev = 0;
-  bool destroyed = false;
-  bool lost = false;
-  std::string lost_msg;
-  cudaStream_t s_step = nullptr, s_copy = nullptr;
-  ahx_dims dims{};
-  int esize = 4, px = 0;
-  uint32_t ps = 0, qs = 0;
-  void* f[2] = {nullptr, nullptr};
-  void* g[2] = {nullptr, nullptr};
-  unsigned char* d_params = nullptr;
-  uint4* d_colv = nullptr;
-  uint32_t* d_ktop = nullptr;
-  uint32_t* d_oldk = nullptr;
-  float4* d_dbg = nullptr;
-  double* d_budget = nullptr;
-  bool budget_on = false;
-  StatsScratch* d_stats = nullptr;
-  int parity = 0;
-  int64_t steps = 0;
-  int block_y = 4, zslab = 0, minb = 0;
-  int tma_ty = 0, tma_depth = 0;          // staged kernel selected when tma_ty > 0
-  bool maps_ok = false;
-  TmaMaps maps[2][2];                     // [TY 4 / 8][parity]: tensor maps of the state read by a step
-  int* d_err = nullptr;                   // error word the staged kernel sets
-  ReadSlot reads[AHX_MAX_READS];
-  uint64_t next_read = 0;
-  UploadSlot up[kUploadSlots];
-  int up_next = 0;
-  std::vector<Fence> fences;
-  uint64_t next_fence = 0;
-  char name[64] = {0};
-};
-
-namespace {
-
 // mark the handle lost on a CUDA error; returns AHX_EDEVICE with the message
-ahx_status cuda_fail(ahx_handle* h, cudaError_t e, const char* what) {
+ahx_status ahx::cuda_fail(ahx_handle* h, cudaError_t e, const char* what) {
   std::string m = std::string(what) + ": " + cudaGetErrorString(e);
   if (h) {
     h->lost = true;
@@ -117,26 +51,24 @@ ahx_status cuda_fail(ahx_handle* h, cudaError_t e, const char* what) {
     if (e__ != cudaSuccess) return cuda_fail(h, e__, #call); \
   } while (0)
 
-ahx_status check(ahx_handle* h) {
+ahx_status ahx::check(ahx_handle* h) {
   if (!h) return fail(AHX_EINVAL, "live solver: null handle");
   if (h->destroyed) return fail(AHX_EDESTROYED, "live solver: destroyed");
   if (h->lost) return fail(AHX_EDEVICE, "live solver: CUDA device lost (" + h->lost_msg + ")");
+  if (h->batch_lost.load()) return fail(AHX_EDEVICE, "live solver: CUDA device lost (a batched step failed)");
   return AHX_OK;
 }
 
-size_t nxy(const ahx_handle* h) { return (size_t)h->dims.nx * h->dims.ny; }
-size_t ncells(const ahx_handle* h) { return nxy(h) * h->dims.nz; }
-size_t params_bytes(const ahx_handle* h) { return 64 + 16 * (size_t)h->dims.nz; }
-
-DomainView view(ahx_handle* h) {
+// the view of the handle's state for a step that reads buffer `parity`
+DomainView ahx::view_at(ahx_handle* h, int parity) {
   DomainView D;
   D.params = h->d_params;
   D.colv = h->d_colv;
   D.ktop = h->d_ktop;
-  D.fA = h->f[h->parity];
-  D.fB = h->f[1 - h->parity];
-  D.gA = h->g[h->parity];
-  D.gB = h->g[1 - h->parity];
+  D.fA = h->f[parity];
+  D.fB = h->f[1 - parity];
+  D.gA = h->g[parity];
+  D.gB = h->g[1 - parity];
   D.dbg = h->d_dbg;
   D.budget = h->d_budget;
   D.err = h->d_err;
@@ -149,6 +81,14 @@ DomainView view(ahx_handle* h) {
   set_offsets(D);
   return D;
 }
+
+namespace {
+
+size_t nxy(const ahx_handle* h) { return (size_t)h->dims.nx * h->dims.ny; }
+size_t ncells(const ahx_handle* h) { return nxy(h) * h->dims.nz; }
+size_t params_bytes(const ahx_handle* h) { return 64 + 16 * (size_t)h->dims.nz; }
+
+DomainView view(ahx_handle* h) { return view_at(h, h->parity); }
 
 using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                    const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
@@ -277,8 +217,10 @@ void free_all(ahx_handle* h) {
   h->s_step = h->s_copy = nullptr;
 }
 
+}  // namespace
+
 // bounded wait on an event; the handle lock is not held while waiting
-ahx_status wait_event(ahx_handle* h, cudaEvent_t ev, int timeout_ms) {
+ahx_status ahx::wait_event(ahx_handle* h, cudaEvent_t ev, int timeout_ms) {
   const auto t0 = std::chrono::steady_clock::now();
   int spin = 0;
   for (;;) {
@@ -294,8 +236,6 @@ ahx_status wait_event(ahx_handle* h, cudaEvent_t ev, int timeout_ms) {
     else std::this_thread::sleep_for(std::chrono::microseconds(50));
   }
 }
-
-}  // namespace
 
 extern "C" {
 
@@ -393,6 +333,8 @@ ahx_status ahx_destroy(ahx_handle* h) {
   {
     std::lock_guard<std::mutex> lk(h->mu);
     if (h->destroyed) return AHX_OK;
+    if (h->batch_refs > 0)
+      return fail(AHX_EINVAL, "live solver: the handle belongs to a batch; destroy the batch first");
     h->destroyed = true;
     free_all(h);
   }

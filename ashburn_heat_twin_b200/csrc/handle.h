@@ -1,0 +1,96 @@
+// Internal state of a live-solver handle, shared by the C ABI translation units (api.cu, batch.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdint>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "ahx.h"
+#include "launch.h"
+
+namespace ahx {
+
+constexpr int kUploadSlots = 4;
+// column levels (kt, ktop) are validated against this bound so every level index stays a small non-negative int
+constexpr uint32_t kMaxLevel = 65535;
+
+struct ReadSlot {
+  bool busy = false;
+  uint64_t ticket = 0;
+  int nzv = 0, want_vol = 0, want_wind = 0;
+  float* d_surf = nullptr;     // 3*NXY
+  uint32_t* d_vol = nullptr;   // ceil(nz*NXY/4)
+  unsigned* d_tmax = nullptr;
+  float* h_surf = nullptr;     // pinned
+  uint8_t* h_vol = nullptr;    // pinned
+  unsigned* h_tmax = nullptr;  // pinned
+  cudaEvent_t ev_kernels = nullptr, ev_done = nullptr;
+};
+
+struct UploadSlot {
+  void* h = nullptr;   // pinned
+  size_t bytes = 0;
+  cudaEvent_t ev = nullptr;
+  bool used = false;
+};
+
+struct Fence {
+  uint64_t ticket;
+  cudaEvent_t ev;
+};
+
+}  // namespace ahx
+
+struct ahx_handle {
+  std::mutex mu;
+  int dev = 0;
+  bool destroyed = false;
+  bool lost = false;
+  std::string lost_msg;
+  cudaStream_t s_step = nullptr, s_copy = nullptr;
+  ahx_dims dims{};
+  int esize = 4, px = 0;
+  uint32_t ps = 0, qs = 0;
+  void* f[2] = {nullptr, nullptr};
+  void* g[2] = {nullptr, nullptr};
+  unsigned char* d_params = nullptr;
+  uint4* d_colv = nullptr;
+  uint32_t* d_ktop = nullptr;
+  uint32_t* d_oldk = nullptr;
+  float4* d_dbg = nullptr;
+  double* d_budget = nullptr;
+  bool budget_on = false;
+  ahx::StatsScratch* d_stats = nullptr;
+  int parity = 0;
+  int64_t steps = 0;
+  int block_y = 4, zslab = 0, minb = 0;
+  int tma_ty = 0, tma_depth = 0;          // staged kernel selected when tma_ty > 0
+  bool maps_ok = false;
+  ahx::TmaMaps maps[2][2];                     // [TY 4 / 8][parity]: tensor maps of the state read by a step
+  int* d_err = nullptr;                   // error word the staged kernel sets
+  ahx::ReadSlot reads[AHX_MAX_READS];
+  uint64_t next_read = 0;
+  ahx::UploadSlot up[ahx::kUploadSlots];
+  int up_next = 0;
+  std::vector<ahx::Fence> fences;
+  uint64_t next_fence = 0;
+  char name[64] = {0};
+  int batch_refs = 0;                     // batches this handle belongs to (it cannot be destroyed meanwhile)
+  std::atomic<int> batch_lost{0};         // set (without the lock) when a batched step over this handle failed
+};
+
+
+namespace ahx {
+
+// helpers of api.cu that batch.cu uses
+ahx_status fail(ahx_status st, const std::string& msg);                      // sets ahx_last_error()
+ahx_status cuda_fail(ahx_handle* h, cudaError_t e, const char* what);       // marks h lost (if non-null)
+ahx_status check(ahx_handle* h);                                             // null / destroyed / lost
+DomainView view_at(ahx_handle* h, int parity);                               // the state read at this parity
+ahx_status wait_event(ahx_handle* h, cudaEvent_t ev, int timeout_ms);        // bounded, lock not held
+
+}  // namespace ahx

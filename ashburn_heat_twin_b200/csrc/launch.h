@@ -23,13 +23,32 @@ struct StepLaunch {
   const TmaMaps* maps = nullptr;   // tensor maps of the state being read
 };
 
+// one tile of a batched step: block (bx, by, bz) of member `member`'s 32 x 4 x zslab decomposition
+struct BatchTile {
+  uint16_t member, bx, by, bz;
+};
+
+struct BatchLaunch {
+  int precision;                 // ahx_precision, the same for every member
+  int minb;                      // 4 / 5 / 6 resident 128-thread blocks per SM
+  int max_nz;                    // largest member nz (sizes the staged inflow profile)
+  int grid;                      // persistent blocks
+  int ntiles;
+  const DomainView* views;       // device: one view per member
+  const BatchTile* tiles;        // device: ntiles tiles, member-major
+  const int* zslabs;             // device: z-slab depth per member
+};
+
 // fused step, IEEE-exact arithmetic (step_exact.cu, built with -fmad=false)
 namespace exact {
 cudaError_t launch_step(const DomainView& D, const StepLaunch& L, cudaStream_t s);
+// with occupancy != nullptr: only report resident blocks per SM for this configuration
+cudaError_t launch_batch(const BatchLaunch& B, cudaStream_t s, int* occupancy);
 }
 // fused step, contracted arithmetic (step_fast.cu, built with -fmad=true)
 namespace fast {
 cudaError_t launch_step(const DomainView& D, const StepLaunch& L, cudaStream_t s);
+cudaError_t launch_batch(const BatchLaunch& B, cudaStream_t s, int* occupancy);
 }
 
 // aux.cu

@@ -27,6 +27,56 @@ __global__ void __launch_bounds__(32 * TY, TY == 4 ? 4 : 2)
   step_tma_block<S, AHX_STEP_FAST != 0, TY, DEPTH>(D, M, zslab);
 }
 
+// Batched step: one persistent launch steps every member domain of a batch. Tile t (32 x 4 columns x that member's
+// z-slab) is taken by block t mod gridDim.x, in order; each tile copies its member's view to shared memory and runs
+// the same step_block as a solo launch, so a member's result is bit-identical to stepping it alone.
+template <class S, int MINB>
+__global__ void __launch_bounds__(128, MINB) batch_kernel(const DomainView* __restrict__ views,
+                                                          const BatchTile* __restrict__ tiles,
+                                                          const int* __restrict__ zslabs, int ntiles) {
+  __shared__ DomainView sD;
+  __shared__ int s_zslab;
+  static_assert(sizeof(DomainView) % 4 == 0, "the view copies as 32-bit words");
+  const int tid = threadIdx.y * 32 + threadIdx.x;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const BatchTile T = tiles[t];
+    const int* src = reinterpret_cast<const int*>(views + T.member);
+    int* dst = reinterpret_cast<int*>(&sD);
+    for (int w = tid; w < (int)(sizeof(DomainView) / 4); w += 128) dst[w] = src[w];
+    if (tid == 0) s_zslab = zslabs[T.member];
+    __syncthreads();
+    step_block<S, 0, false, AHX_STEP_FAST != 0>(sD, T.bx, T.by, T.bz, s_zslab);
+    __syncthreads();   // the next tile overwrites the view and the staged profile
+  }
+}
+
+template <class S, int MINB>
+static cudaError_t batch_t(const BatchLaunch& B, cudaStream_t s, int* occupancy) {
+  const size_t smem = (size_t)B.max_nz * sizeof(float4);
+  if (occupancy) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occupancy, batch_kernel<S, MINB>, 128, smem);
+  batch_kernel<S, MINB><<<B.grid, dim3(32, 4), smem, s>>>(B.views, B.tiles, B.zslabs, B.ntiles);
+  return cudaGetLastError();
+}
+
+template <class S>
+static cudaError_t batch_s(const BatchLaunch& B, cudaStream_t s, int* occupancy) {
+  switch (B.minb) {
+    case 4: return batch_t<S, 4>(B, s, occupancy);
+    case 6: return batch_t<S, 6>(B, s, occupancy);
+    default: return batch_t<S, 5>(B, s, occupancy);
+  }
+}
+
+cudaError_t launch_batch(const BatchLaunch& B, cudaStream_t s, int* occupancy) {
+  switch (B.precision) {
+    case 0: return batch_s<float>(B, s, occupancy);
+    case 1: return batch_s<__half>(B, s, occupancy);
+    case 2: return batch_s<__nv_bfloat16>(B, s, occupancy);
+    case 3: return batch_s<double>(B, s, occupancy);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
 template <class S, int TY, int DEPTH>
 static cudaError_t launch_tma_t(const DomainView& D, const StepLaunch& L, cudaStream_t s) {
   const int zs = L.zslab > 0 ? L.zslab : D.nz;

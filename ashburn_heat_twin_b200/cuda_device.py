@@ -24,7 +24,9 @@ SYMBOLS = ('ahx_create', 'ahx_destroy', 'ahx_last_error', 'ahx_get_info', 'ahx_s
            'ahx_set_ktop', 'ahx_init_flow', 'ahx_clear_heat', 'ahx_set_parity', 'ahx_step', 'ahx_sync', 'ahx_fence',
            'ahx_fence_query', 'ahx_read_submit', 'ahx_read_wait', 'ahx_read_state', 'ahx_write_state',
            'ahx_read_state_f64', 'ahx_write_state_f64', 'ahx_read_dbg', 'ahx_clear_dbg', 'ahx_stats',
-           'ahx_budget_enable', 'ahx_budget_read', 'ahx_set_launch', 'ahx_autotune', 'ahx_time_steps', 'ahx_stats_noalloc')
+           'ahx_budget_enable', 'ahx_budget_read', 'ahx_set_launch', 'ahx_autotune', 'ahx_time_steps', 'ahx_stats_noalloc',
+           'ahx_batch_create', 'ahx_batch_step', 'ahx_batch_time_steps', 'ahx_batch_sync', 'ahx_batch_set_variant',
+           'ahx_batch_get_info', 'ahx_batch_destroy')
 
 
 class AhxError(RuntimeError):
@@ -55,6 +57,12 @@ class BudgetOut(ctypes.Structure):
     _fields_ = [('theta_sum', ctypes.c_double), ('src_sum', ctypes.c_double),
                 ('face_theta_u', ctypes.c_double * 4), ('face_u', ctypes.c_double * 4), ('cells', ctypes.c_double),
                 ('pad', ctypes.c_double * 5)]
+
+
+class BatchInfoOut(ctypes.Structure):
+    _fields_ = [('members', ctypes.c_int32), ('tiles', ctypes.c_int32), ('grid', ctypes.c_int32),
+                ('minb', ctypes.c_int32), ('use_graph', ctypes.c_int32), ('pad', ctypes.c_int32),
+                ('cells', ctypes.c_int64)]
 
 
 _lib = None
@@ -100,6 +108,13 @@ def load_library(path: str = LIB_PATH):
         'ahx_autotune': [H, i, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
                          ctypes.POINTER(ctypes.c_float)],
         'ahx_stats_noalloc': [i, i, i, vp, vp, vp, vp, vp],
+        'ahx_batch_create': [ctypes.POINTER(H), i, ctypes.POINTER(H)],
+        'ahx_batch_step': [H, i],
+        'ahx_batch_time_steps': [H, i, i, ctypes.POINTER(ctypes.c_float)],
+        'ahx_batch_sync': [H, i],
+        'ahx_batch_set_variant': [H, i, i],
+        'ahx_batch_get_info': [H, ctypes.POINTER(BatchInfoOut)],
+        'ahx_batch_destroy': [H],
     }
     for name, args in sig.items():
         fn = getattr(L, name)
@@ -311,7 +326,57 @@ class CudaDevice:
 
     def destroy(self):
         if self.hd is not None:
-            try:
-                self.hd.call('ahx_destroy')
-            finally:
-                self.hd = None
+            self.hd.call('ahx_destroy')   # refused while the handle belongs to a batch
+            self.hd = None
+
+
+class Batch:
+    """Owner of one ahx_batch over the handles of several CudaDevice backends (same device, precision and
+    arithmetic; grids may differ): each step of all members is one persistent launch, replayed from a CUDA graph."""
+
+    def __init__(self, devices):
+        self.L = load_library()
+        self.devices = list(devices)
+        arr = (ctypes.c_void_p * len(self.devices))(*[d.hd.h.value for d in self.devices])
+        b = ctypes.c_void_p()
+        self._call('ahx_batch_create', arr, len(self.devices), ctypes.byref(b))
+        self.b = b
+
+    def _call(self, name, *args):
+        st = getattr(self.L, name)(*args)
+        if st != 0:
+            msg = self.L.ahx_last_error().decode(errors='replace')
+            raise AhxError(st, msg or f'{name}: {STATUS.get(st, st)}')
+        return st
+
+    def _flip(self, n):
+        for d in self.devices:
+            d._p ^= (int(n) & 1)
+
+    def step(self, n):
+        self._call('ahx_batch_step', self.b, int(n))
+        self._flip(n)
+
+    def time_steps(self, n, timeout_s=None):
+        """n batched steps between two CUDA events on the batch stream; returns their device time in ms"""
+        ms = ctypes.c_float()
+        self._call('ahx_batch_time_steps', self.b, int(n), -1 if timeout_s is None else int(timeout_s * 1000),
+                   ctypes.byref(ms))
+        self._flip(n)
+        return ms.value
+
+    def sync(self, timeout_s=None):
+        self._call('ahx_batch_sync', self.b, -1 if timeout_s is None else int(timeout_s * 1000))
+
+    def set_variant(self, minb=0, use_graph=True):
+        self._call('ahx_batch_set_variant', self.b, int(minb), 1 if use_graph else 0)
+
+    def info(self):
+        o = BatchInfoOut()
+        self._call('ahx_batch_get_info', self.b, ctypes.byref(o))
+        return {k: getattr(o, k) for k, _ in BatchInfoOut._fields_ if k != 'pad'}
+
+    def destroy(self):
+        if self.b is not None:
+            self._call('ahx_batch_destroy', self.b)
+            self.b = None

@@ -331,11 +331,10 @@ class LiveSolver:
     def destroy(self):
         if self._destroyed:
             return
+        if self._dev is not None:
+            self._dev.destroy()     # raises, and the solver stays usable, while it belongs to a live batch
         self._destroyed = True
-        try:
-            self._dev.destroy()
-        finally:
-            self._dev = None
+        self._dev = None
 
     # ------------------------------------------------------------------ validation hooks (solver.js:496-578)
     @property
@@ -481,3 +480,67 @@ def create_live_solver(backend=None, **opts):
 
 # the reference's spelling
 createLiveSolver = create_live_solver
+
+
+class LiveBatch:
+    """Steps several live solvers together: one persistent launch per step for all of them, replayed two steps at a
+    time from a CUDA graph (libahx ahx_batch_*). No counterpart in the reference, which runs one solver per device;
+    each member's state after batch.step(n) is bit-identical to member.step(n).
+
+    Members must use the CUDA backend with the same device, precision and arithmetic; their grids may differ. They
+    stay fully usable on their own (setMet, setExistingFlux, read, step ...), ordered against the batch's steps. A
+    member cannot be destroyed while it belongs to a live batch: destroy the batch first."""
+
+    def __init__(self, solvers):
+        from .cuda_device import Batch, CudaDevice
+        self.solvers = list(solvers)
+        if not self.solvers:
+            raise LiveSolverError('live solver: a batch needs at least one solver')
+        for s in self.solvers:
+            s._check()
+            if not isinstance(s._dev, CudaDevice):
+                raise LiveSolverError('live solver: batched stepping needs the CUDA backend')
+        try:
+            self._b = Batch([s._dev for s in self.solvers])
+        except Exception as e:
+            raise LiveSolverError(str(e)) from None
+
+    @property
+    def info(self):
+        return self._b.info()
+
+    def _advance(self, n):
+        for s in self.solvers:
+            s._n += n
+            s._steps += n
+            s._advanceFlowRef(n)
+
+    def step(self, n=1):
+        """queue n steps of every member; the Pending resolves when the device has finished them."""
+        n = max(0, int(math.floor(n)))
+        if self._b is None:
+            return Pending(value=None, error=LiveSolverError('live solver: batch destroyed'))
+        try:
+            if n > 0:
+                self._b.step(n)
+        except Exception as e:
+            return Pending(value=None, error=LiveSolverError(str(e)))
+        self._advance(n)
+        # every member's stream waits for the batch, so a fence on one member resolves after the batched steps
+        return self.solvers[0]._dev.fence()
+
+    def benchmark(self, n=50):
+        """n batched steps timed on the device; returns aggregate MLUPS over all members' cells."""
+        n = max(1, int(n))
+        ms = self._b.time_steps(n)
+        self._advance(n)
+        return self._b.info()['cells'] * n / (ms * 1e-3) / 1e6
+
+    def set_variant(self, minb=0, use_graph=True):
+        self._b.set_variant(minb, use_graph)
+
+    def destroy(self):
+        """release the batch (idempotent); the members stay alive."""
+        if self._b is not None:
+            self._b.destroy()
+            self._b = None

@@ -203,6 +203,34 @@ ahx_status ahx_autotune(ahx_handle* h, int steps_per_trial, int* best_block_y, i
 ahx_status ahx_stats_noalloc(int nx, int ny, int nz, const float* f, const float* g, const uint32_t* ktop,
                              ahx_stats_out* out, void* stream);
 
+/* --- batched stepping ----------------------------------------------------------------------------------------- */
+
+/* No counterpart in the reference, which steps one domain per device (solver.js:401-427). A batch groups handles of
+ * one device, precision and arithmetic (grids may differ) so that each step of all of them is ONE persistent launch
+ * (a member's result is bit-identical to stepping it alone), replayed two steps at a time from a CUDA graph. Members
+ * stay usable on their own (parameters, columns, reads, solo steps): the batch's launches are ordered after the work
+ * already queued on each member's stream and before anything queued there later. A member cannot be destroyed while
+ * it belongs to a batch (AHX_EINVAL), and batched steps do not accumulate budgets (members with budgets enabled are
+ * rejected). Each member's tiles are 32 x 4 columns x its z-slab (ahx_set_launch / ahx_autotune; 16 levels when
+ * unset); the register-budget variant is the members' tuned one when they agree, else 5. */
+typedef struct ahx_batch ahx_batch;
+
+typedef struct {
+  int members, tiles, grid, minb, use_graph, pad;
+  int64_t cells;   /* sum of nx*ny*nz over the members */
+} ahx_batch_info_out;
+
+ahx_status ahx_batch_create(ahx_handle* const* members, int count, ahx_batch** out);
+/* n steps of every member, asynchronous; each member's step count and parity advance as with ahx_step */
+ahx_status ahx_batch_step(ahx_batch* b, int n);
+/* n batched steps timed with CUDA events on the batch stream; waits at most timeout_ms (< 0: no bound) */
+ahx_status ahx_batch_time_steps(ahx_batch* b, int n, int timeout_ms, float* ms);
+ahx_status ahx_batch_sync(ahx_batch* b, int timeout_ms);
+/* register-budget variant 4 / 5 / 6 (0 = keep) and whether steps replay the captured graph (1) or launch (0) */
+ahx_status ahx_batch_set_variant(ahx_batch* b, int minb, int use_graph);
+ahx_status ahx_batch_get_info(ahx_batch* b, ahx_batch_info_out* out);
+ahx_status ahx_batch_destroy(ahx_batch* b);   /* idempotent; members are released */
+
 #ifdef __cplusplus
 }
 #endif
