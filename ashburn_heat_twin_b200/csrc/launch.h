@@ -31,12 +31,12 @@ struct BatchTile {
 struct BatchLaunch {
   int precision;                 // ahx_precision, the same for every member
   int minb;                      // 4 / 5 / 6 resident 128-thread blocks per SM
-  int max_nz;                    // largest member nz (sizes the staged inflow profile)
+  int max_nz;                    // level capacity (sizes the staged inflow profile in shared memory)
   int grid;                      // persistent blocks
-  int ntiles;
   const DomainView* views;       // device: one view per member
-  const BatchTile* tiles;        // device: ntiles tiles, member-major
+  const BatchTile* tiles;        // device: *ntiles tiles, member-major
   const int* zslabs;             // device: z-slab depth per member
+  const int* ntiles;             // device: tile count
 };
 
 // fused step, IEEE-exact arithmetic (step_exact.cu, built with -fmad=false)

@@ -29,15 +29,18 @@ __global__ void __launch_bounds__(32 * TY, TY == 4 ? 4 : 2)
 
 // Batched step: one persistent launch steps every member domain of a batch. Tile t (32 x 4 columns x that member's
 // z-slab) is taken by block t mod gridDim.x, in order; each tile copies its member's view to shared memory and runs
-// the same step_block as a solo launch, so a member's result is bit-identical to stepping it alone.
+// the same step_block as a solo launch, so a member's result is bit-identical to stepping it alone. The tile count
+// is read from device memory, so one captured launch serves any membership the tables describe.
 template <class S, int MINB>
 __global__ void __launch_bounds__(128, MINB) batch_kernel(const DomainView* __restrict__ views,
                                                           const BatchTile* __restrict__ tiles,
-                                                          const int* __restrict__ zslabs, int ntiles) {
+                                                          const int* __restrict__ zslabs,
+                                                          const int* __restrict__ ntiles_ptr) {
   __shared__ DomainView sD;
   __shared__ int s_zslab;
   static_assert(sizeof(DomainView) % 4 == 0, "the view copies as 32-bit words");
   const int tid = threadIdx.y * 32 + threadIdx.x;
+  const int ntiles = *ntiles_ptr;
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const BatchTile T = tiles[t];
     const int* src = reinterpret_cast<const int*>(views + T.member);

@@ -25,8 +25,8 @@ SYMBOLS = ('ahx_create', 'ahx_destroy', 'ahx_last_error', 'ahx_get_info', 'ahx_s
            'ahx_fence_query', 'ahx_read_submit', 'ahx_read_wait', 'ahx_read_state', 'ahx_write_state',
            'ahx_read_state_f64', 'ahx_write_state_f64', 'ahx_read_dbg', 'ahx_clear_dbg', 'ahx_stats',
            'ahx_budget_enable', 'ahx_budget_read', 'ahx_set_launch', 'ahx_autotune', 'ahx_time_steps', 'ahx_stats_noalloc',
-           'ahx_batch_create', 'ahx_batch_step', 'ahx_batch_time_steps', 'ahx_batch_sync', 'ahx_batch_set_variant',
-           'ahx_batch_get_info', 'ahx_batch_destroy')
+           'ahx_batch_create', 'ahx_batch_step', 'ahx_batch_time_steps', 'ahx_batch_sync', 'ahx_batch_set_launch',
+           'ahx_batch_get_info', 'ahx_batch_destroy', 'ahx_batch_set_members')
 
 
 class AhxError(RuntimeError):
@@ -61,7 +61,7 @@ class BudgetOut(ctypes.Structure):
 
 class BatchInfoOut(ctypes.Structure):
     _fields_ = [('members', ctypes.c_int32), ('tiles', ctypes.c_int32), ('grid', ctypes.c_int32),
-                ('minb', ctypes.c_int32), ('use_graph', ctypes.c_int32), ('pad', ctypes.c_int32),
+                ('minb', ctypes.c_int32), ('use_graph', ctypes.c_int32), ('zslab_max', ctypes.c_int32),
                 ('cells', ctypes.c_int64)]
 
 
@@ -112,7 +112,8 @@ def load_library(path: str = LIB_PATH):
         'ahx_batch_step': [H, i],
         'ahx_batch_time_steps': [H, i, i, ctypes.POINTER(ctypes.c_float)],
         'ahx_batch_sync': [H, i],
-        'ahx_batch_set_variant': [H, i, i],
+        'ahx_batch_set_launch': [H, i, i, i],
+        'ahx_batch_set_members': [H, ctypes.POINTER(H), i],
         'ahx_batch_get_info': [H, ctypes.POINTER(BatchInfoOut)],
         'ahx_batch_destroy': [H],
     }
@@ -256,17 +257,33 @@ class CudaDevice:
                 int(want_wind), ctypes.byref(t))
         ticket = t.value
         NXY = self.nx * self.ny
+        got = {}
 
-        def wait(timeout_s):
+        def fetch(timeout_ms):
+            """copy the read-back out once it has arrived; False if it has not within timeout_ms"""
             surf = np.empty(NXY, np.float32)
             u = np.empty(NXY, np.float32) if want_wind else None
             v = np.empty(NXY, np.float32) if want_wind else None
             vb = np.empty(nzv * NXY, np.uint8) if want_vol else None
             tm = np.zeros(1, np.float32)
-            self._c('ahx_read_wait', ctypes.c_uint64(ticket), -1 if timeout_s is None else int(timeout_s * 1000),
-                    _ptr(surf), _ptr(u), _ptr(v), _ptr(vb), _ptr(tm))
-            return finish((surf, u, v, vb, float(tm[0])))
-        return Pending(poll=lambda: False, wait=wait)
+            try:
+                self._c('ahx_read_wait', ctypes.c_uint64(ticket), int(timeout_ms), _ptr(surf), _ptr(u), _ptr(v),
+                        _ptr(vb), _ptr(tm))
+            except AhxError as e:
+                if e.status == 5 and timeout_ms >= 0:    # not arrived yet: the read stays pending
+                    return False
+                raise
+            got['res'] = finish((surf, u, v, vb, float(tm[0])))
+            return True
+
+        def poll():
+            return 'res' in got or fetch(0)
+
+        def wait(timeout_s):
+            if 'res' not in got and not fetch(-1 if timeout_s is None else int(timeout_s * 1000)):
+                raise AhxError(5, 'live solver: timed out waiting for the GPU')
+            return got['res']
+        return Pending(poll=poll, wait=wait)
 
     def read_state(self):
         f = np.empty(19 * self.N, np.float32)
@@ -368,13 +385,18 @@ class Batch:
     def sync(self, timeout_s=None):
         self._call('ahx_batch_sync', self.b, -1 if timeout_s is None else int(timeout_s * 1000))
 
-    def set_variant(self, minb=0, use_graph=True):
-        self._call('ahx_batch_set_variant', self.b, int(minb), 1 if use_graph else 0)
+    def set_launch(self, minb=0, zslab=0, use_graph=True):
+        self._call('ahx_batch_set_launch', self.b, int(minb), int(zslab), 1 if use_graph else 0)
+
+    def set_members(self, devices):
+        self.devices = list(devices)
+        arr = (ctypes.c_void_p * max(1, len(self.devices)))(*[d.hd.h.value for d in self.devices])
+        self._call('ahx_batch_set_members', self.b, arr, len(self.devices))
 
     def info(self):
         o = BatchInfoOut()
         self._call('ahx_batch_get_info', self.b, ctypes.byref(o))
-        return {k: getattr(o, k) for k, _ in BatchInfoOut._fields_ if k != 'pad'}
+        return {k: getattr(o, k) for k, _ in BatchInfoOut._fields_}
 
     def destroy(self):
         if self.b is not None:

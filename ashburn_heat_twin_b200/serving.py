@@ -1,0 +1,327 @@
+"""Serving loop with continuous batching over the live solver.
+
+A request is one scenario of the live page (js/live.js drives one at a time: setMet, setExistingFlux,
+setNewCampuses, then step until a simulated time, then read()). The server runs many at once on one device:
+
+- admission: an arrived request takes a solver slot of its grid class (a recycled one, or a new one while the
+  device-memory budget allows) as long as the resident cells stay under `max_cells`; otherwise it queues (FIFO);
+- a slot is configured exactly like a fresh page would be: setMet, setExistingFlux, setNewCampuses, resetFlow;
+- the active slots are stepped together by one LiveBatch (one persistent launch per step, CUDA-graph replay) in
+  chunks of at most `chunk` steps, never past any member's remaining steps; the member list follows the active
+  slots at chunk boundaries (continuous batching) through a stream-ordered table update;
+- chunks are queued ahead (up to `depth` in flight) so admission, set-up uploads and read-back overlap the device;
+- a finished request is answered with read() (surface theta, u, v and the u8 volume) and its slot returns to the
+  pool of its class once that read has arrived.
+
+Each request's answer is bit-identical to running its scenario alone on a fresh solver (the batched step is).
+The reference has no server; this is the host-side scheduler over the batched C ABI (ahx_batch_*).
+"""
+from __future__ import annotations
+
+import math
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import solver as S
+
+
+@dataclass
+class Request:
+    id: int
+    arrival: float            # seconds after the trace start
+    dx: float
+    heightM: float
+    met: dict
+    flux: float
+    campus: dict
+    sim_s: float = 600.0
+    steps: int = 0            # filled at admission from the slot's dt
+    cells: int = 0            # nx * ny * nz of the request's grid, filled at admission
+    # filled by the server
+    admitted: float = math.nan
+    done: float = math.nan
+    result: dict = field(default=None, repr=False)
+
+
+class _Slot:
+    def __init__(self, solver, key):
+        self.solver = solver
+        self.key = key
+        self.req = None
+        self.left = 0
+        self.bytes = 0
+
+
+def _state_bytes(solver):
+    try:
+        return int(solver._dev.info()['state_bytes'])
+    except Exception:
+        return solver.info['nCells'] * 52 * 4
+
+
+class Server:
+    """Continuous-batching server on one device. `backend` builds a solver's device (CudaDevice by default);
+    `batch_factory(solvers)` returns an object with step(n) -> Pending, set_members(solvers) and destroy()
+    (LiveBatch by default)."""
+
+    def __init__(self, static, backend=None, batch_factory=None, max_cells=64_000_000, chunk=64, u10Max=8.0,
+                 hbm_budget_bytes=None, depth=2, clock=time.perf_counter, sleep=time.sleep):
+        self.static = static
+        self.backend = backend
+        self.batch_factory = batch_factory or S.LiveBatch
+        self.max_cells = int(max_cells)
+        self.chunk = int(chunk)
+        self.depth = max(1, int(depth))
+        self.u10Max = u10Max
+        self.hbm_budget = hbm_budget_bytes
+        self.clock, self.sleep = clock, sleep
+        self.pool: dict = {}          # grid class -> idle slots
+        self.slots: list = []         # every slot created
+        self.active: list = []
+        self.batch = None
+        self.batch_members = None
+        self.bytes_used = 0
+        self.cell_updates = 0
+        self.launch_chunks = 0
+        self.rebuilds = 0
+        self.evictions = 0
+        self.batch_steps = 0
+
+    # ---------------------------------------------------------------- slots
+    def _new_solver(self, r: Request):
+        return S.create_live_solver(backend=self.backend, static=self.static, dx=r.dx, allowAnyDx=True,
+                                    heightM=r.heightM, u10Max=self.u10Max, met=r.met, existingFlux=r.flux)
+
+    def _take_slot(self, r: Request):
+        key = (r.dx, r.heightM)
+        idle = self.pool.get(key)
+        if idle:
+            return idle.pop()
+        if self.hbm_budget is not None:
+            need = self._class_cells(r) * self._bytes_per_cell()
+            while self.bytes_used + need > self.hbm_budget and self._evict_idle():
+                pass
+            if self.bytes_used + need > self.hbm_budget and self.slots:
+                return None
+        s = self._new_solver(r)
+        slot = _Slot(s, key)
+        slot.bytes = _state_bytes(s)
+        self.bytes_used += slot.bytes
+        self.slots.append(slot)
+        return slot
+
+    def prewarm(self, template: Request, n: int):
+        """create n idle slots of template's grid class up front (solver, device buffers, read-back staging), as a
+        server keeps a warm pool; stops early when the memory budget is reached."""
+        made = 0
+        for _ in range(int(n)):
+            if self.hbm_budget is not None and self.slots:
+                need = self._class_cells(template) * self._bytes_per_cell()
+                if self.bytes_used + need > self.hbm_budget:
+                    break
+            s = self._new_solver(template)
+            slot = _Slot(s, (template.dx, template.heightM))
+            slot.bytes = _state_bytes(s)
+            self.bytes_used += slot.bytes
+            self.slots.append(slot)
+            self.pool.setdefault(slot.key, []).append(slot)
+            made += 1
+        return made
+
+    def _bytes_per_cell(self):
+        for sl in self.slots:
+            return sl.bytes / sl.solver.info['nCells']
+        return 208.0
+
+    def _evict_idle(self):
+        """free one idle slot of any class (idle slots are never batch members: the member list follows the active
+        slots as soon as requests finish)."""
+        for key, idle in self.pool.items():
+            if idle:
+                sl = idle.pop()
+                sl.solver.destroy()
+                self.slots.remove(sl)
+                self.bytes_used -= sl.bytes
+                self.evictions += 1
+                return True
+        return False
+
+    def _configure(self, slot: _Slot, r: Request):
+        s = slot.solver
+        s.setMet(r.met)
+        s.setExistingFlux(r.flux)
+        s.setNewCampuses([r.campus])
+        s.resetFlow()
+        r.steps = int(math.ceil(r.sim_s / s.info['dt'] - 1e-9))
+        r.cells = int(s.info['nCells'])
+        slot.req, slot.left = r, r.steps
+
+    def _cells(self):
+        return sum(sl.solver.info['nCells'] for sl in self.active)
+
+    def _class_cells(self, r: Request):
+        idle = self.pool.get((r.dx, r.heightM))
+        if idle:
+            return idle[-1].solver.info['nCells']
+        for sl in self.slots:
+            if sl.key == (r.dx, r.heightM):
+                return sl.solver.info['nCells']
+        nx = int(round(6000 / r.dx))
+        return nx * nx * int(round(r.heightM / r.dx))
+
+    # ---------------------------------------------------------------- batch
+    def _sync_members(self):
+        """keep the batch's member list equal to the active slots (stream-ordered; no synchronisation)."""
+        members = [sl.solver for sl in self.active]
+        if self.batch_members == members:
+            return
+        if self.batch is None:
+            if not members:
+                return
+            self.batch = self.batch_factory(members)
+        else:
+            self.batch.set_members(members)
+        self.batch_members = members
+        self.rebuilds += 1
+
+    def _poll(self, draining, done, t0, block=False):
+        """retire finished requests whose read-back has arrived (all of them when block)."""
+        keep = []
+        for sl, p in draining:
+            if block or p.done():
+                sl.req.result = p.result()
+                sl.req.done = self.clock() - t0
+                done.append(sl.req)
+                sl.req = None
+                self.pool.setdefault(sl.key, []).append(sl)
+            else:
+                keep.append((sl, p))
+        draining[:] = keep
+
+    # ---------------------------------------------------------------- main loop
+    def run(self, requests, timeout_s=None):
+        """Serve `requests` in real time (arrival times relative to the call); returns the statistics dict. Raises
+        TimeoutError if the trace is not finished within timeout_s seconds (None: no bound)."""
+        reqs = sorted(requests, key=lambda r: r.arrival)
+        queue: list = []
+        nxt = 0
+        t0 = self.clock()
+        done: list = []
+        inflight: list = []      # fences of queued chunks, oldest first
+        draining: list = []      # (slot, read Pending) of finished requests
+        while len(done) < len(reqs):
+            now = self.clock() - t0
+            if timeout_s is not None and now > timeout_s:
+                raise TimeoutError(f'serving: {len(done)} of {len(reqs)} requests answered after {now:.1f} s')
+            while nxt < len(reqs) and reqs[nxt].arrival <= now:
+                queue.append(reqs[nxt])
+                nxt += 1
+            # admission (FIFO) while cells and memory allow; the first request is always admitted
+            while queue:
+                r = queue[0]
+                if self.active and self._cells() + self._class_cells(r) > self.max_cells:
+                    break
+                slot = self._take_slot(r)
+                if slot is None:
+                    break
+                queue.pop(0)
+                self._configure(slot, r)
+                r.admitted = self.clock() - t0
+                self.active.append(slot)
+            if self.active:
+                self._sync_members()
+                k = min(self.chunk, min(sl.left for sl in self.active))
+                inflight.append(self.batch.step(k))
+                self.launch_chunks += 1
+                self.batch_steps += k
+                self.cell_updates += k * self._cells()
+                finished = [sl for sl in self.active if sl.left == k]
+                for sl in self.active:
+                    sl.left -= k
+                for sl in finished:
+                    # ordered after this chunk on the member's own stream
+                    draining.append((sl, sl.solver.read(vol=True, wind=True)))
+                    self.active.remove(sl)
+                if finished:
+                    self._sync_members()   # leavers are released now, so idle slots can be evicted safely
+            # keep at most `depth` chunks queued; retire read-backs while waiting
+            while inflight and (len(inflight) > self.depth or not self.active):
+                if inflight[0].done():
+                    inflight.pop(0).result()
+                    continue
+                if timeout_s is not None and self.clock() - t0 > timeout_s:
+                    raise TimeoutError(f'serving: a chunk did not finish within {timeout_s} s')
+                self._poll(draining, done, t0)
+                self.sleep(0.0002)
+            self._poll(draining, done, t0)
+            if not self.active:
+                if draining:
+                    self.sleep(0.0002)
+                elif not queue and nxt < len(reqs):
+                    self.sleep(max(0.0, min(0.01, reqs[nxt].arrival - (self.clock() - t0))))
+        for p in inflight:
+            p.result()
+        makespan = self.clock() - t0
+        return self._stats(reqs, makespan)
+
+    def _stats(self, reqs, makespan):
+        lat = np.array([r.done - r.arrival for r in reqs])
+        qd = np.array([r.admitted - r.arrival for r in reqs])
+        upd = self.cell_updates
+        return dict(requests=len(reqs), makespan_s=makespan, cell_updates=int(upd),
+                    glups=upd / makespan / 1e9 if makespan > 0 else 0.0,
+                    latency_p50_s=float(np.percentile(lat, 50)), latency_p99_s=float(np.percentile(lat, 99)),
+                    latency_mean_s=float(lat.mean()), queue_p50_s=float(np.percentile(qd, 50)),
+                    queue_p99_s=float(np.percentile(qd, 99)), chunks=self.launch_chunks, batch_rebuilds=self.rebuilds,
+                    slots=len(self.slots), slot_bytes=self.bytes_used, evictions=self.evictions,
+                    batch_steps=self.batch_steps)
+
+    def close(self):
+        if self.batch is not None:
+            self.batch.destroy()
+            self.batch = None
+        self.batch_members = None
+        for sl in self.slots:
+            sl.solver.destroy()
+        self.slots, self.pool, self.active = [], {}, []
+
+
+def requests_from_trace(trace, sim_s=600.0):
+    """scenarios.serve_trace entries -> Request objects."""
+    return [Request(id=t['id'], arrival=t['arrival'], dx=t['dx'], heightM=t['heightM'], met=dict(t['met']),
+                    flux=t['flux'], campus=t['campus'], sim_s=sim_s) for t in trace]
+
+
+def fifo_serial(requests, seconds_of):
+    """Latencies of the same requests solved one after another in arrival order (a single FIFO server whose service
+    time for request r is seconds_of(r)); returns (latencies, makespan)."""
+    t = 0.0
+    lat = []
+    start = min(r.arrival for r in requests)
+    for r in sorted(requests, key=lambda r: r.arrival):
+        t = max(t, r.arrival) + seconds_of(r)
+        lat.append(t - r.arrival)
+    return np.array(lat), t - start
+
+
+class SequentialBatch:
+    """A stand-in batch that steps each member on its own (for backends without batched stepping, e.g. the CPU
+    oracle in host-logic tests); same step(n) -> Pending / set_members / destroy() protocol as LiveBatch."""
+
+    def __init__(self, solvers):
+        self.solvers = list(solvers)
+
+    def set_members(self, solvers):
+        self.solvers = list(solvers)
+
+    def step(self, n):
+        p = S.Pending(value=None)
+        for s in self.solvers:
+            p = s.step(n)
+            p.result()
+        return p
+
+    def destroy(self):
+        self.solvers = []

@@ -509,6 +509,20 @@ class LiveBatch:
     def info(self):
         return self._b.info()
 
+    def set_members(self, solvers):
+        """replace the member list (possibly empty); ordered after the batch's queued steps, no synchronisation."""
+        from .cuda_device import CudaDevice
+        solvers = list(solvers)
+        for s in solvers:
+            s._check()
+            if not isinstance(s._dev, CudaDevice):
+                raise LiveSolverError('live solver: batched stepping needs the CUDA backend')
+        try:
+            self._b.set_members([s._dev for s in solvers])
+        except Exception as e:
+            raise LiveSolverError(str(e)) from None
+        self.solvers = solvers
+
     def _advance(self, n):
         for s in self.solvers:
             s._n += n
@@ -521,10 +535,12 @@ class LiveBatch:
         if self._b is None:
             return Pending(value=None, error=LiveSolverError('live solver: batch destroyed'))
         try:
-            if n > 0:
+            if n > 0 and self.solvers:
                 self._b.step(n)
         except Exception as e:
             return Pending(value=None, error=LiveSolverError(str(e)))
+        if not self.solvers:
+            return Pending(value=None)
         self._advance(n)
         # every member's stream waits for the batch, so a fence on one member resolves after the batched steps
         return self.solvers[0]._dev.fence()
@@ -536,8 +552,25 @@ class LiveBatch:
         self._advance(n)
         return self._b.info()['cells'] * n / (ms * 1e-3) / 1e6
 
-    def set_variant(self, minb=0, use_graph=True):
-        self._b.set_variant(minb, use_graph)
+    def set_launch(self, minb=0, zslab=0, use_graph=True):
+        """register-budget variant (4 / 5 / 6, 0 = keep), tile depth (levels, 0 = keep, -1 = automatic) and graph
+        replay on or off."""
+        self._b.set_launch(minb, zslab, use_graph)
+
+    def autotune(self, steps_per_trial=4):
+        """time the register-budget variants x tile depths on the batch itself and keep the fastest. Like
+        benchmark(), the trials advance every member's state (by 9 x (2 + steps_per_trial) steps)."""
+        best = None
+        for minb in (4, 5, 6):
+            for zs in (-1, 16, 8):
+                self._b.set_launch(minb, zs, True)
+                self._b.time_steps(2)
+                ms = self._b.time_steps(steps_per_trial)
+                self._advance(2 + steps_per_trial)
+                if best is None or ms < best[0]:
+                    best = (ms, minb, zs)
+        self._b.set_launch(best[1], best[2], True)
+        return dict(minb=best[1], zslab=best[2], ms_per_step=best[0] / steps_per_trial)
 
     def destroy(self):
         """release the batch (idempotent); the members stay alive."""

@@ -19,6 +19,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -36,6 +37,12 @@ WORKLOADS = {
                     '60 DC roofs', dx=30, heightM=960, met='C1_MET', spec='C1'),
     'c2q': dict(desc='300x300x64 cells at 10 m (5.76 M), synthetic seed 3: 6 hills 0-40 m, 1000 buildings, '
                      '53 DC roofs', dx=10, heightM=640, met='C2_MET', spec='C2Q'),
+    'c4': dict(desc='64 domains in one batch: 32 x 200x200x32 at 30 m + 32 x 150x150x24 at 40 m (58.2 M cells), '
+                    'synthetic seed 1 box; per domain seeded wind (U[0,360) deg, U[2,8] m/s), roof flux U[200,600] '
+                    'W/m2 and one 120 MW campus (300 x 300 m hall) at a building-free site', spec='C1'),
+    'c5': dict(desc='serving: Poisson arrivals of live-solver requests, 40 % 150x150x24 at 40 m, 40 % 200x200x32 at '
+                    '30 m, 20 % 300x300x48 at 20 m, 10 simulated minutes each (1,754 / 2,338 / 3,507 steps), seeded '
+                    'wind, roof flux and one 120 MW campus per request, synthetic seed 1 box', spec='C1'),
 }
 METRIC = 'GLUPS (all cells) of the fused D3Q19+D3Q7 step, 600x600x64'
 
@@ -170,6 +177,207 @@ def run_reference(a, rank):
     return 0
 
 
+def main_batch(a, rank, world, local, dist, torch):
+    """The batched workload: 64 seeded domains stepped by one persistent launch per step (a CUDA graph replays two
+    steps); launch shapes tuned per grid class on scratch copies, then the batch's own variant and tile depth.
+    Reports the aggregate rate, the same members stepped one after another (serial) for comparison, and an
+    end-to-end frame rate through the public API."""
+    from ashburn_heat_twin_b200 import LiveBatch
+    from ashburn_heat_twin_b200 import scenarios as SC
+    from ashburn_heat_twin_b200 import solver as S
+    from ashburn_heat_twin_b200 import synth
+    from ashburn_heat_twin_b200.cuda_device import CudaDevice
+    st = synth.make_static10(synth.C1)
+    scen = SC.batch64(st)
+
+    def backend(nx, ny, nz):
+        return CudaDevice(nx, ny, nz, device=local, precision=a.precision, arith=a.arith)
+
+    solvers = []
+    for c in scen:
+        s = S.create_live_solver(backend=backend, static=st, dx=c['dx'], heightM=c['heightM'], u10Max=8,
+                                 met=c['met'], existingFlux=c['flux'])
+        s.setNewCampuses([c['campus']])
+        solvers.append(s)
+    classes = {}
+    for s in solvers:
+        classes.setdefault((s.info['nx'], s.info['ny'], s.info['nz']), []).append(s)
+    tuned = {}
+    for key, members in classes.items():
+        if a.no_autotune:
+            break
+        by, zs, ms = members[0]._dev.autotune(3)
+        for m in members[1:]:
+            m._dev.set_launch(by, zs)
+        tuned['x'.join(map(str, key))] = dict(block_y=by, zslab=zs, ms=round(ms, 4))
+        log(f'[rank {rank}] autotune {key}: block_y {by} zslab {zs} {ms:.3f} ms/step')
+    cells = sum(s.info['nCells'] for s in solvers)
+    fluid = sum(s.info['nFluid'] for s in solvers)
+    b = LiveBatch(solvers)
+    btune = None
+    if not a.no_autotune:
+        btune = b.autotune(4)
+        log(f'[rank {rank}] batch autotune: {btune}')
+    b._b.time_steps(a.warmup)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize(local)
+
+    barrier()
+    with Clocks(local) as clk:
+        barrier()
+        ms = b._b.time_steps(a.steps)
+        barrier()
+    clocks = clk.summary()
+    ms_all = ms
+    if dist is not None:
+        t = torch.tensor([ms], device=f'cuda:{local}', dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_all = float(t.item())
+    value = world * cells * a.steps / (ms_all / 1e3) / 1e9
+    # the same members stepped one after another with their own tuned launches (no batch)
+    serial_ms = sum(s._dev.time_steps(a.steps) for s in solvers)
+    esize = {'fp32': 4, 'fp16': 2, 'bf16': 2, 'fp64': 8}[a.precision]
+    bytes_launch = fluid * 52 * esize
+    launch_ms = ms / a.steps
+    achieved = bytes_launch / (launch_ms / 1e3) / 1e9
+    peak, peak_kind = measured_peaks()
+    roof = dict(bound='hbm', achieved=achieved, peak=peak, unit='GB/s', frac=achieved / peak, traffic=None,
+                peak_source=peak_kind, bytes_per_launch=bytes_launch, launch_ms=launch_ms,
+                kernel='batch_kernel (one persistent launch per step over all 64 domains)')
+    # end to end: per frame every member gets a new parameter block, the batch steps F, every member is read
+    F = a.frame
+    frames = max(3, a.steps // 4)
+    mets = [dict(c['met']) for c in scen]
+    b.step(F).result()
+    barrier()
+    t0 = time.perf_counter()
+    h2d = d2h = 0
+    for fr in range(frames):
+        for s, m in zip(solvers, mets):
+            m['u10'] = min(8.0, m['u10'] + 0.01)
+            s.setMet(m)
+            h2d += len(s._params)
+        b.step(F)
+        pend = [s.read(vol=False, wind=True) for s in solvers]
+        for s, p in zip(solvers, pend):
+            p.result()
+            d2h += 3 * s.info['nx'] * s.info['ny'] * 4 + 4
+    barrier()
+    e2e_s = time.perf_counter() - t0
+    if dist is not None:
+        t = torch.tensor([e2e_s], device=f'cuda:{local}', dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = dict(value=world * cells * F * frames / e2e_s / 1e9, unit='GLUPS', h2d_bytes_per_step=h2d / (F * frames),
+               d2h_bytes_per_step=d2h / (F * frames), frame_steps=F, frames=frames,
+               per_frame='setMet on all 64 members (parameter blocks H2D) + batch step(F) + read(wind) of every member '
+                         '(surface theta, u, v D2H)')
+    info = b.info
+    b.destroy()
+    for s in solvers:
+        s.destroy()
+    out = dict(metric='GLUPS (all cells) of the batched fused D3Q19+D3Q7 step, 64 domains (32 x 200x200x32 + '
+                      '32 x 150x150x24)', value=value, unit='GLUPS', n_gpus=world, steps=a.steps, warmup=a.warmup,
+               ms_per_step=ms_all / a.steps, higher_is_better=True, scaling='weak', vs_baseline=None,
+               dtype={'fp32': 'f32', 'fp16': 'f16-store/f32', 'bf16': 'bf16-store/f32', 'fp64': 'f64'}[a.precision],
+               data='synthetic (seeded terrain, buildings and scenarios; no public dataset involved)',
+               config=dict(workload=WORKLOADS['c4']['desc'], precision=a.precision, arith=a.arith, scheme='pull',
+                           parallelism=f'replicas x{world}', cells=cells, fluid_cells=fluid,
+                           l2=f'state {cells * 52 * esize / 1e9:.1f} GB vs 126 MB L2', tuned=tuned,
+                           batch=dict(tiles=info['tiles'], grid=info['grid'], minb=info['minb'],
+                                      zslab_max=info['zslab_max'], graph=bool(info['use_graph']), tuned=btune)),
+               serial=dict(value=world * cells * a.steps / (serial_ms / 1e3) / 1e9, unit='GLUPS',
+                           ms_per_step=serial_ms / a.steps, what='the 64 members stepped one after another, each '
+                                                                 'with its own tuned launch'),
+               roofline=roof, cpu_baseline=None, e2e=e2e, gpu_launches=a.steps, clocks=clocks,
+               glups_fluid=world * fluid * a.steps / (ms_all / 1e3) / 1e9)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    return 0
+
+
+def main_serve(a, rank, world, local, dist, torch):
+    """The serving workload: a seeded Poisson trace of requests served with continuous batching (one persistent
+    launch per step over all admitted requests, chunks of --chunk steps, admission under a cell budget). Reports the
+    aggregate served rate, latency percentiles and queueing delay, and the same trace solved back to back (FIFO, each
+    request alone at its class's measured solo rate)."""
+    import numpy as np
+
+    from ashburn_heat_twin_b200 import scenarios as SC
+    from ashburn_heat_twin_b200 import serving as SV
+    from ashburn_heat_twin_b200 import synth
+    from ashburn_heat_twin_b200.cuda_device import CudaDevice
+    st = synth.make_static10(synth.C1)
+
+    def backend(nx, ny, nz):
+        return CudaDevice(nx, ny, nz, device=local, precision=a.precision, arith=a.arith)
+
+    # warm pool: idle slots of every class in the mix's proportions up to the cell budget, then a short trace
+    # through the same server (kernels, graph capture, read-back staging)
+    srv = SV.Server(st, backend=backend, max_cells=a.max_cells, chunk=a.chunk)
+    per_req = sum(sh * (6000 // dx) ** 2 * round(hm / dx) for sh, dx, hm in SC.SERVE_MIX)
+    for sh, dx, hm in SC.SERVE_MIX:
+        tmpl = SV.Request(id=-1, arrival=0.0, dx=dx, heightM=hm, met=dict(synth.C1_MET), flux=400.0,
+                          campus=dict(id='W', mw=0.0, halls=[]))
+        srv.prewarm(tmpl, int(math.ceil(sh * a.max_cells / per_req)) + 1)
+    warm = SV.requests_from_trace(SC.serve_trace(st, 6, 1000.0, seed=a.seed + 100), sim_s=5.0)
+    srv.run(warm, timeout_s=300)
+    srv.cell_updates = srv.launch_chunks = srv.rebuilds = srv.evictions = srv.batch_steps = 0
+    reqs = SV.requests_from_trace(SC.serve_trace(st, a.requests, a.rate, seed=a.seed), sim_s=SC.SERVE_SIM_S)
+    with Clocks(local) as clk:
+        stats = srv.run(reqs, timeout_s=900)
+    clocks = clk.summary()
+    # solo rate per grid class (one of the server's own slots, its launch tuned on a scratch copy)
+    rate = {}
+    for key, idle in srv.pool.items():
+        s = idle[0].solver
+        s._dev.autotune(3)
+        ms = s._dev.time_steps(20)
+        rate[key] = s.info['nCells'] * 20 / (ms / 1e3)
+    lat_ser, mk_ser = SV.fifo_serial(reqs, lambda r: r.steps * r.cells / rate[(r.dx, r.heightM)])
+    upd = stats['cell_updates']
+    h2d = sum(64 + 16 * int(round(r.heightM / r.dx)) + 20 * (6000 // int(r.dx)) ** 2 for r in reqs)
+    d2h = sum((3 * 4 + min(int(round(r.heightM / r.dx)), int(round(420 / r.dx)))) * (6000 // int(r.dx)) ** 2
+              for r in reqs)
+    steps_total = sum(r.steps for r in reqs)
+    classes = {f'{int(k[0])} m': dict(solo_glups=v / 1e9) for k, v in rate.items()}
+    srv.close()
+    out = dict(metric='GLUPS (all cells) served with continuous batching, Poisson trace of live-solver requests',
+               value=stats['glups'], unit='GLUPS', n_gpus=world, steps=stats['batch_steps'], warmup=6,
+               ms_per_step=stats['makespan_s'] * 1e3 / max(1, stats['batch_steps']), higher_is_better=True,
+               scaling='weak', vs_baseline=None,
+               dtype={'fp32': 'f32', 'fp16': 'f16-store/f32', 'bf16': 'bf16-store/f32', 'fp64': 'f64'}[a.precision],
+               data='synthetic (seeded terrain, buildings and request trace; no public dataset involved)',
+               config=dict(workload=WORKLOADS['c5']['desc'], requests=a.requests, rate_hz=a.rate, seed=a.seed,
+                           precision=a.precision, arith=a.arith, max_cells=a.max_cells, chunk=a.chunk,
+                           parallelism=f'replicas x{world}', classes=classes,
+                           l2='per-step state of the admitted requests >> 126 MB L2'),
+               serving=dict(latency_p50_s=stats['latency_p50_s'], latency_p99_s=stats['latency_p99_s'],
+                            latency_mean_s=stats['latency_mean_s'], queue_p50_s=stats['queue_p50_s'],
+                            queue_p99_s=stats['queue_p99_s'], makespan_s=stats['makespan_s'],
+                            cell_updates=upd, chunks=stats['chunks'], batch_updates=stats['batch_rebuilds'],
+                            slots=stats['slots']),
+               serial=dict(value=upd / mk_ser / 1e9, unit='GLUPS', latency_p50_s=float(np.percentile(lat_ser, 50)),
+                           latency_p99_s=float(np.percentile(lat_ser, 99)), makespan_s=mk_ser,
+                           what='the same trace solved back to back in arrival order, each request alone at its '
+                                'class solo device rate (host work not counted)'),
+               roofline=None, cpu_baseline=None,
+               e2e=dict(value=stats['glups'], unit='GLUPS', h2d_bytes_per_step=h2d / steps_total,
+                        d2h_bytes_per_step=d2h / steps_total,
+                        what='the served rate is end to end: request set-up uploads, batched steps and read() '
+                             'downloads are all inside the wall-clock makespan'),
+               gpu_launches=stats['batch_steps'], clocks=clocks)
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
@@ -184,7 +392,13 @@ def main():
     ap.add_argument('--block-y', type=int, default=0, help='fix the launch shape instead of autotuning')
     ap.add_argument('--zslab', type=int, default=0)
     ap.add_argument('--workload', default='c2', choices=sorted(WORKLOADS),
-                    help='c2 (the benchmark) or c1 (a smaller case for profiling)')
+                    help='c2 (the benchmark), c1 / c2q (smaller cases for profiling), c4 (64 domains in one batch), '
+                         'c5 (serving)')
+    ap.add_argument('--requests', type=int, default=48, help='serving: requests in the trace')
+    ap.add_argument('--rate', type=float, default=50.0, help='serving: mean arrival rate (requests/s)')
+    ap.add_argument('--seed', type=int, default=5, help='serving: trace seed')
+    ap.add_argument('--max-cells', type=int, default=64_000_000, help='serving: resident cell budget')
+    ap.add_argument('--chunk', type=int, default=64, help='serving: steps per batched chunk')
     a = ap.parse_args()
     a.warmup = max(a.warmup, 3)
 
@@ -205,6 +419,10 @@ def main():
                                 device_id=torch.device('cuda', local))
     from ashburn_heat_twin_b200 import _build
     _build.build()
+    if a.workload == 'c4':
+        return main_batch(a, rank, world, local, dist, torch)
+    if a.workload == 'c5':
+        return main_serve(a, rank, world, local, dist, torch)
     s = make_solver(device=local, precision=a.precision, arith=a.arith, workload=a.workload)
     dev = s._dev
     nx, ny, nz = s.info['nx'], s.info['ny'], s.info['nz']

@@ -211,23 +211,31 @@ ahx_status ahx_stats_noalloc(int nx, int ny, int nz, const float* f, const float
  * stay usable on their own (parameters, columns, reads, solo steps): the batch's launches are ordered after the work
  * already queued on each member's stream and before anything queued there later. A member cannot be destroyed while
  * it belongs to a batch (AHX_EINVAL), and batched steps do not accumulate budgets (members with budgets enabled are
- * rejected). Each member's tiles are 32 x 4 columns x its z-slab (ahx_set_launch / ahx_autotune; 16 levels when
- * unset); the register-budget variant is the members' tuned one when they agree, else 5. */
+ * rejected). Tiles are 32 x 4 columns by whole columns when the batch is large enough (at least 4 tiles per
+ * persistent block), else by each member's z-slab (ahx_set_launch / ahx_autotune; 16 levels when unset); the
+ * register-budget variant is the members' tuned one when they agree, else 5. ahx_batch_set_launch overrides both. */
 typedef struct ahx_batch ahx_batch;
 
 typedef struct {
-  int members, tiles, grid, minb, use_graph, pad;
+  int members, tiles, grid, minb, use_graph, zslab_max;
   int64_t cells;   /* sum of nx*ny*nz over the members */
 } ahx_batch_info_out;
 
 ahx_status ahx_batch_create(ahx_handle* const* members, int count, ahx_batch** out);
+/* replace the member list (count >= 0; same device, precision and arithmetic); stream-ordered after the batch's
+ * earlier steps, without synchronising or allocating unless the batch outgrows its tables; the captured graph stays
+ * valid. Members that leave are released (they may then be destroyed: their streams already wait for the batched
+ * steps that used them). */
+ahx_status ahx_batch_set_members(ahx_batch* b, ahx_handle* const* members, int count);
 /* n steps of every member, asynchronous; each member's step count and parity advance as with ahx_step */
 ahx_status ahx_batch_step(ahx_batch* b, int n);
 /* n batched steps timed with CUDA events on the batch stream; waits at most timeout_ms (< 0: no bound) */
 ahx_status ahx_batch_time_steps(ahx_batch* b, int n, int timeout_ms, float* ms);
 ahx_status ahx_batch_sync(ahx_batch* b, int timeout_ms);
-/* register-budget variant 4 / 5 / 6 (0 = keep) and whether steps replay the captured graph (1) or launch (0) */
-ahx_status ahx_batch_set_variant(ahx_batch* b, int minb, int use_graph);
+/* launch set-up: register-budget variant 4 / 5 / 6 (0 = keep); tile depth zslab in levels for every member (clipped
+ * to its nz; 0 = keep; -1 = automatic: whole columns when that leaves at least 4 tiles per persistent block, else each
+ * member's own z-slab); whether steps replay the captured graph (1) or launch one kernel per step (0) */
+ahx_status ahx_batch_set_launch(ahx_batch* b, int minb, int zslab, int use_graph);
 ahx_status ahx_batch_get_info(ahx_batch* b, ahx_batch_info_out* out);
 ahx_status ahx_batch_destroy(ahx_batch* b);   /* idempotent; members are released */
 

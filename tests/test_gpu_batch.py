@@ -67,7 +67,7 @@ def test_batch_matches_solo(precision, arith):
     for a, m in zip(solo, mem):
         same(a, m)
     # the plain-launch path gives the same bits as the graph
-    b.set_variant(use_graph=False)
+    b.set_launch(use_graph=False)
     for s in solo:
         s.step(5).result()
     b.step(5).result()
@@ -84,11 +84,11 @@ def test_batch_variants_agree():
     mem = [scenario(i) for i in range(3)]
     ref = [scenario(i) for i in range(3)]
     b = LiveBatch(mem)
-    b.set_variant(minb=4)
+    b.set_launch(minb=4, zslab=8)
     b.step(4).result()
     b.destroy()
     b2 = LiveBatch(ref)
-    b2.set_variant(minb=6)
+    b2.set_launch(minb=6, zslab=-1)
     b2.step(4).result()
     b2.destroy()
     for a, m in zip(ref, mem):
@@ -112,3 +112,26 @@ def test_batch_membership_rules():
     a.destroy()
     c.destroy()
     h.destroy()
+
+
+def test_batch_membership_changes_match_solo():
+    solo = [scenario(i, 'fp32', 'fast') for i in range(3)]
+    mem = [scenario(i, 'fp32', 'fast') for i in range(3)]
+    b = LiveBatch(mem[:2])
+    b.step(5)
+    b.set_members([mem[1], mem[2]])      # member 0 leaves, member 2 joins: no synchronisation in between
+    b.step(4)
+    b.set_members([mem[2], mem[0], mem[1]])
+    b.step(3).result()
+    for s, n in zip(solo, (8, 12, 7)):
+        s.step(n).result()
+    for a, m in zip(solo, mem):
+        same(a, m)
+    b.set_members([mem[1]])
+    mem[0].destroy()                     # a member that left may be destroyed while the batch lives
+    b.step(2).result()
+    solo[1].step(2).result()
+    same(solo[1], mem[1])
+    b.destroy()
+    for s in solo + mem[1:]:
+        s.destroy()
