@@ -42,14 +42,14 @@ struct ahx_batch {
   std::mutex mu;
   bool destroyed = false, lost = false;
   std::string lost_msg;
-  int dev = 0, precision = 0, arith = 0, minb = 5, nsm = 0, occ = 0, grid = 0;
+  int dev = 0, precision = 0, arith = 0, minb = 4, nsm = 0, occ = 0, grid = 0;
   int cap_members = 0, cap_nz = 0;
   int64_t cap_tiles = 0;
   std::vector<ahx_handle*> members;
   std::vector<int> zslab;          // tile depth per member
   std::vector<int> base_parity;    // each member's parity when the view table was written
   int phase = 0;                   // steps since then, mod 2
-  int zs_policy = -1;              // tile-depth policy (build_plan)
+  int zs_policy = 8;               // tile-depth policy (build_plan)
   int ntiles = 0;
   int64_t cells = 0;
   cudaStream_t s = nullptr;
@@ -57,6 +57,7 @@ struct ahx_batch {
   BatchTile* d_tiles = nullptr;
   int* d_zslab = nullptr;
   int* d_ntiles = nullptr;
+  int* d_sched = nullptr;          // tile counter and finished-block counter of the running launch
   Staging stage[2];
   int stage_next = 0;
   cudaEvent_t ev_done = nullptr;
@@ -100,6 +101,7 @@ BatchLaunch launch_args(const ahx_batch* b, int set) {
   L.tiles = b->d_tiles;
   L.zslabs = b->d_zslab;
   L.ntiles = b->d_ntiles;
+  L.sched = b->d_sched;
   return L;
 }
 
@@ -135,6 +137,8 @@ void free_tables(ahx_batch* b) {
   if (b->d_tiles) cudaFree(b->d_tiles);
   if (b->d_zslab) cudaFree(b->d_zslab);
   if (b->d_ntiles) cudaFree(b->d_ntiles);
+  if (b->d_sched) cudaFree(b->d_sched);
+  b->d_sched = nullptr;
   b->d_views = nullptr;
   b->d_tiles = nullptr;
   b->d_zslab = nullptr;
@@ -166,11 +170,12 @@ ahx_status ensure_capacity(ahx_batch* b, int members, int64_t tiles, int nz) {
   if (cudaMalloc(&b->d_views, 2 * (size_t)cm * sizeof(DomainView)) != cudaSuccess ||
       cudaMalloc(&b->d_tiles, (size_t)ct * sizeof(BatchTile)) != cudaSuccess ||
       cudaMalloc(&b->d_zslab, (size_t)cm * sizeof(int)) != cudaSuccess ||
-      cudaMalloc(&b->d_ntiles, sizeof(int)) != cudaSuccess) {
+      cudaMalloc(&b->d_ntiles, sizeof(int)) != cudaSuccess || cudaMalloc(&b->d_sched, 2 * sizeof(int)) != cudaSuccess) {
     cudaGetLastError();
     free_tables(b);
     return fail(AHX_ENOMEM, "live solver: batch table allocation failed");
   }
+  AHX_BCUDA(b, cudaMemsetAsync(b->d_sched, 0, 2 * sizeof(int), b->s));
   for (Staging& g : b->stage) {
     if (cudaMallocHost(&g.views, 2 * (size_t)cm * sizeof(DomainView)) != cudaSuccess ||
         cudaMallocHost(&g.tiles, (size_t)ct * sizeof(BatchTile)) != cudaSuccess ||
@@ -197,8 +202,9 @@ ahx_status ensure_capacity(ahx_batch* b, int members, int64_t tiles, int nz) {
   return AHX_OK;
 }
 
-// Tile plan for depth policy `policy` (> 0: that depth for every member, clipped to its nz; -1: whole columns when
-// that still gives at least 4 tiles per persistent block, else each member's own z-slab or 16 levels).
+// Tile plan for depth policy `policy` (> 0: that depth for every member, clipped to its nz, 8 levels by default;
+// -1: whole columns when that still gives at least 4 tiles per persistent block, else each member's own z-slab or
+// 16 levels).
 ahx_status build_plan(const std::vector<ahx_handle*>& mem, int policy, int grid, std::vector<BatchTile>& tiles,
                       std::vector<int>& zslab) {
   auto own = [](const ahx_handle* h) {
@@ -356,7 +362,7 @@ ahx_status ahx_batch_create(ahx_handle* const* members, int count, ahx_batch** o
   }
   std::vector<ahx_handle*> mem(members, members + count);
   MemberLocks lock(mem);
-  // register-budget variant: the members' tuned choice when they agree, else 5 (96 registers)
+  // register-budget variant: the members' tuned choice when they agree, else 4 (128 registers)
   std::vector<int> minbs;
   for (const ahx_handle* h : mem)
     if (h->minb > 0) minbs.push_back(h->minb);

@@ -37,6 +37,7 @@ struct BatchLaunch {
   const BatchTile* tiles;        // device: *ntiles tiles, member-major
   const int* zslabs;             // device: z-slab depth per member
   const int* ntiles;             // device: tile count
+  int* sched;                    // device: [next tile, blocks done], zero between launches
 };
 
 // fused step, IEEE-exact arithmetic (step_exact.cu, built with -fmad=false)

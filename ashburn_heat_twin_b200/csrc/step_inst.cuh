@@ -27,21 +27,27 @@ __global__ void __launch_bounds__(32 * TY, TY == 4 ? 4 : 2)
   step_tma_block<S, AHX_STEP_FAST != 0, TY, DEPTH>(D, M, zslab);
 }
 
-// Batched step: one persistent launch steps every member domain of a batch. Tile t (32 x 4 columns x that member's
-// z-slab) is taken by block t mod gridDim.x, in order; each tile copies its member's view to shared memory and runs
-// the same step_block as a solo launch, so a member's result is bit-identical to stepping it alone. The tile count
-// is read from device memory, so one captured launch serves any membership the tables describe.
+// Batched step: one persistent launch steps every member domain of a batch. Blocks take tiles (32 x 4 columns x that
+// member's z-slab) from a device counter in list order until the list is exhausted, so unequal tiles balance; each
+// tile copies its member's view to shared memory and runs the same step_block as a solo launch, so a member's
+// result is bit-identical to stepping it alone. The tile count is read from device memory, so one captured launch
+// serves any membership the tables describe. The last block to finish resets the counters for the next launch on
+// the stream (launches on one stream do not overlap).
 template <class S, int MINB>
 __global__ void __launch_bounds__(128, MINB) batch_kernel(const DomainView* __restrict__ views,
                                                           const BatchTile* __restrict__ tiles,
                                                           const int* __restrict__ zslabs,
-                                                          const int* __restrict__ ntiles_ptr) {
+                                                          const int* __restrict__ ntiles_ptr, int* sched) {
   __shared__ DomainView sD;
-  __shared__ int s_zslab;
+  __shared__ int s_zslab, s_t;
   static_assert(sizeof(DomainView) % 4 == 0, "the view copies as 32-bit words");
   const int tid = threadIdx.y * 32 + threadIdx.x;
   const int ntiles = *ntiles_ptr;
-  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+  for (;;) {
+    if (tid == 0) s_t = atomicAdd(&sched[0], 1);
+    __syncthreads();
+    const int t = s_t;
+    if (t >= ntiles) break;
     const BatchTile T = tiles[t];
     const int* src = reinterpret_cast<const int*>(views + T.member);
     int* dst = reinterpret_cast<int*>(&sD);
@@ -49,7 +55,14 @@ __global__ void __launch_bounds__(128, MINB) batch_kernel(const DomainView* __re
     if (tid == 0) s_zslab = zslabs[T.member];
     __syncthreads();
     step_block<S, 0, false, AHX_STEP_FAST != 0>(sD, T.bx, T.by, T.bz, s_zslab);
-    __syncthreads();   // the next tile overwrites the view and the staged profile
+    __syncthreads();   // the next tile overwrites the view, the staged profile and s_t
+  }
+  if (tid == 0) {
+    __threadfence();
+    if (atomicAdd(&sched[1], 1) == (int)gridDim.x - 1) {
+      atomicExch(&sched[0], 0);
+      atomicExch(&sched[1], 0);
+    }
   }
 }
 
@@ -57,7 +70,7 @@ template <class S, int MINB>
 static cudaError_t batch_t(const BatchLaunch& B, cudaStream_t s, int* occupancy) {
   const size_t smem = (size_t)B.max_nz * sizeof(float4);
   if (occupancy) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occupancy, batch_kernel<S, MINB>, 128, smem);
-  batch_kernel<S, MINB><<<B.grid, dim3(32, 4), smem, s>>>(B.views, B.tiles, B.zslabs, B.ntiles);
+  batch_kernel<S, MINB><<<B.grid, dim3(32, 4), smem, s>>>(B.views, B.tiles, B.zslabs, B.ntiles, B.sched);
   return cudaGetLastError();
 }
 

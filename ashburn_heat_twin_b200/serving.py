@@ -88,6 +88,7 @@ class Server:
         self.rebuilds = 0
         self.evictions = 0
         self.batch_steps = 0
+        self.chunk_log: list = []     # per chunk: [issued s, steps, resident cells, members, finished s (observed)]
 
     # ---------------------------------------------------------------- slots
     def _new_solver(self, r: Request):
@@ -234,6 +235,8 @@ class Server:
                 self._sync_members()
                 k = min(self.chunk, min(sl.left for sl in self.active))
                 inflight.append(self.batch.step(k))
+                self.chunk_log.append([self.clock() - t0, k, self._cells(), len(self.active), math.nan])
+                inflight[-1].log = self.chunk_log[-1]
                 self.launch_chunks += 1
                 self.batch_steps += k
                 self.cell_updates += k * self._cells()
@@ -249,7 +252,10 @@ class Server:
             # keep at most `depth` chunks queued; retire read-backs while waiting
             while inflight and (len(inflight) > self.depth or not self.active):
                 if inflight[0].done():
-                    inflight.pop(0).result()
+                    p = inflight.pop(0)
+                    p.result()
+                    if getattr(p, 'log', None) is not None:
+                        p.log[4] = self.clock() - t0
                     continue
                 if timeout_s is not None and self.clock() - t0 > timeout_s:
                     raise TimeoutError(f'serving: a chunk did not finish within {timeout_s} s')

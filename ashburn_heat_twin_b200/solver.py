@@ -559,10 +559,10 @@ class LiveBatch:
 
     def autotune(self, steps_per_trial=4):
         """time the register-budget variants x tile depths on the batch itself and keep the fastest. Like
-        benchmark(), the trials advance every member's state (by 9 x (2 + steps_per_trial) steps)."""
+        benchmark(), the trials advance every member's state (by 6 x (2 + steps_per_trial) steps)."""
         best = None
-        for minb in (4, 5, 6):
-            for zs in (-1, 16, 8):
+        for minb in (4, 5):
+            for zs in (4, 8, 16):
                 self._b.set_launch(minb, zs, True)
                 self._b.time_steps(2)
                 ms = self._b.time_steps(steps_per_trial)

@@ -330,9 +330,22 @@ def main_serve(a, rank, world, local, dist, torch):
     srv.run(warm, timeout_s=300)
     srv.cell_updates = srv.launch_chunks = srv.rebuilds = srv.evictions = srv.batch_steps = 0
     reqs = SV.requests_from_trace(SC.serve_trace(st, a.requests, a.rate, seed=a.seed), sim_s=SC.SERVE_SIM_S)
+    srv.chunk_log = []
     with Clocks(local) as clk:
         stats = srv.run(reqs, timeout_s=900)
     clocks = clk.summary()
+    # device-busy estimate from the chunk completions the host observed (queue depth keeps the device fed)
+    busy, last = 0.0, 0.0
+    for issued, k, cells_, members, fin in srv.chunk_log:
+        if fin == fin:
+            busy += max(0.0, fin - max(last, issued))
+            last = fin
+    log(f'[rank {rank}] serving: {len(srv.chunk_log)} chunks, observed busy {busy:.2f} s of '
+        f'{stats["makespan_s"]:.2f} s; first chunks: ' +
+        '; '.join(f'{c[1]} steps x {c[2] / 1e6:.1f} M cells ({c[3]} req) {c[0]:.2f}->{c[4]:.2f}s'
+                  for c in srv.chunk_log[:6]) + ' ... last: ' +
+        '; '.join(f'{c[1]} steps x {c[2] / 1e6:.1f} M cells ({c[3]} req) {c[0]:.2f}->{c[4]:.2f}s'
+                  for c in srv.chunk_log[-6:]))
     # solo rate per grid class (one of the server's own slots, its launch tuned on a scratch copy)
     rate = {}
     for key, idle in srv.pool.items():

@@ -211,9 +211,9 @@ ahx_status ahx_stats_noalloc(int nx, int ny, int nz, const float* f, const float
  * stay usable on their own (parameters, columns, reads, solo steps): the batch's launches are ordered after the work
  * already queued on each member's stream and before anything queued there later. A member cannot be destroyed while
  * it belongs to a batch (AHX_EINVAL), and batched steps do not accumulate budgets (members with budgets enabled are
- * rejected). Tiles are 32 x 4 columns by whole columns when the batch is large enough (at least 4 tiles per
- * persistent block), else by each member's z-slab (ahx_set_launch / ahx_autotune; 16 levels when unset); the
- * register-budget variant is the members' tuned one when they agree, else 5. ahx_batch_set_launch overrides both. */
+ * rejected). Tiles are 32 x 4 columns x 8 levels, handed to the persistent blocks from a device counter in list order;
+ * the register-budget variant is the members' tuned one when they agree, else 4. ahx_batch_set_launch overrides
+ * both. */
 typedef struct ahx_batch ahx_batch;
 
 typedef struct {
@@ -233,8 +233,8 @@ ahx_status ahx_batch_step(ahx_batch* b, int n);
 ahx_status ahx_batch_time_steps(ahx_batch* b, int n, int timeout_ms, float* ms);
 ahx_status ahx_batch_sync(ahx_batch* b, int timeout_ms);
 /* launch set-up: register-budget variant 4 / 5 / 6 (0 = keep); tile depth zslab in levels for every member (clipped
- * to its nz; 0 = keep; -1 = automatic: whole columns when that leaves at least 4 tiles per persistent block, else each
- * member's own z-slab); whether steps replay the captured graph (1) or launch one kernel per step (0) */
+ * to its nz; 0 = keep; -1 = whole columns when that leaves at least 4 tiles per persistent block, else each member's
+ * own z-slab); whether steps replay the captured graph (1) or launch one kernel per step (0) */
 ahx_status ahx_batch_set_launch(ahx_batch* b, int minb, int zslab, int use_graph);
 ahx_status ahx_batch_get_info(ahx_batch* b, ahx_batch_info_out* out);
 ahx_status ahx_batch_destroy(ahx_batch* b);   /* idempotent; members are released */
