@@ -37,6 +37,9 @@ WORKLOADS = {
                     '60 DC roofs', dx=30, heightM=960, met='C1_MET', spec='C1'),
     'c2q': dict(desc='300x300x64 cells at 10 m (5.76 M), synthetic seed 3: 6 hills 0-40 m, 1000 buildings, '
                      '53 DC roofs', dx=10, heightM=640, met='C2_MET', spec='C2Q'),
+    'c3': dict(desc='precision study on 600x600x64 at 10 m (config c2): FP32 / FP16 / BF16 storage against the FP64 '
+                    'build, cold start, 2 simulated minutes of spin-up then a 10-minute mean', dx=10, heightM=640,
+               met='C2_MET', spec='C2'),
     'c4': dict(desc='64 domains in one batch: 32 x 200x200x32 at 30 m + 32 x 150x150x24 at 40 m (58.2 M cells), '
                     'synthetic seed 1 box; per domain seeded wind (U[0,360) deg, U[2,8] m/s), roof flux U[200,600] '
                     'W/m2 and one 120 MW campus (300 x 300 m hall) at a building-free site', spec='C1'),
@@ -391,6 +394,99 @@ def main_serve(a, rank, world, local, dist, torch):
     return 0
 
 
+def main_precision(a, rank, world, local, dist, torch):
+    """Storage precision study on the 600x600x64 domain: every storage (FP32, FP16, BF16 with the FMA build; FP64 with
+    the exact build) runs the same cold start for --spin-s simulated seconds, then accumulates the --mean-s mean of
+    theta with the FP64 heat budget fused into the step. Reported per storage against FP64: rel-L2 of the mean
+    near-ground theta (the first fluid cell of every column), peak mean warming, heat-closure terms, the rel-L2 of
+    theta after one step from the FP64 state, and the step rate (GLUPS) on the tuned launch."""
+    import numpy as np
+
+    from ashburn_heat_twin_b200 import params as PM
+    order = ['fp64', 'fp32', 'fp16', 'bf16']
+    sol = {p: make_solver(device=local, precision=p, arith='exact' if p == 'fp64' else 'fast') for p in order}
+    s0 = sol['fp64']
+    nx, ny, nz = s0.info['nx'], s0.info['ny'], s0.info['nz']
+    N = nx * ny * nz
+    dt, dx = s0.info['dt'], s0.info['dx']
+    spin = int(round(a.spin_s / dt))
+    mean = int(round(a.mean_s / dt))
+    ktop = s0._ktopS.astype(np.int64)            # solver orientation, j = 0 south
+    cols = np.nonzero(ktop < nz)[0]
+    first = ktop[cols] * (nx * ny) + cols        # reference-layout index of each column's first fluid cell
+    fluid = (np.arange(nz)[:, None] >= ktop[None, :]).reshape(-1)
+    res = {}
+    for p in order:
+        s = sol[p]
+        dev = s._dev
+        t0 = time.perf_counter()
+        s.step(spin).result()
+        st0 = dev.stats()
+        dev.budget_enable(True)
+        dev.budget_read(reset=True)
+        s._dbg.clearDbg()
+        s._dbg.stepAcc(mean).result()
+        bud = dev.budget_read(reset=True)
+        dev.budget_enable(False)
+        st1 = dev.stats()
+        dbg = s._dbg.readDbg().reshape(N, 4)
+        ng = dbg[first, 0].astype(np.float64) / mean
+        rc = PM.RHO_CP * dx ** 3 / (mean * dt) / 1e6          # K lattice units summed over the window -> MW
+        ftu = bud['face_theta_u']                              # west, east, south, north sums of theta * u_n
+        out_mw = rc * (ftu[1] - ftu[0] + ftu[3] - ftu[2])
+        res[p] = dict(ng=ng, peak=float(ng.max()), injected_mw=rc * bud['src_sum'], advected_out_mw=out_mw,
+                      content_rate_mw=rc * (st1['sumTheta'] - st0['sumTheta']), nonfinite=st1['nonFinite'],
+                      wall_s=time.perf_counter() - t0)
+        log(f'[rank {rank}] precision {p}: {spin}+{mean} steps in {res[p]["wall_s"]:.1f} s, peak {res[p]["peak"]:.4f} K')
+    ref = res['fp64']
+
+    def rel_l2(x, y):
+        return float(np.linalg.norm(x - y) / np.linalg.norm(y))
+
+    # one step from the FP64 state in every storage (theta of the fluid cells)
+    f64, g64 = s0._dev.read_state_f64()
+    s0._dbg.stepOut(1).result()
+    th64 = s0._dbg.readDbg().reshape(N, 4)[fluid, 0].astype(np.float64)
+    step_err = {}
+    for p in order[1:]:
+        sol[p]._dev.write_state(f64.astype(np.float32), g64.astype(np.float32))
+        sol[p]._dbg.stepOut(1).result()
+        th = sol[p]._dbg.readDbg().reshape(N, 4)[fluid, 0].astype(np.float64)
+        step_err[p] = rel_l2(th, th64)
+    # step rate of each storage on its tuned launch (after the study, so the runs share one start)
+    rate = {}
+    for p in order:
+        dev = sol[p]._dev
+        dev.autotune(3)
+        dev.time_steps(a.warmup)
+        ms = dev.time_steps(a.steps)
+        rate[p] = N * a.steps / (ms / 1e3) / 1e9
+    for s in sol.values():
+        s.destroy()
+    prec = {}
+    for p in order:
+        r = res[p]
+        closure = (r['injected_mw'] - r['advected_out_mw'] - r['content_rate_mw']) / r['injected_mw']
+        prec[p] = dict(glups=rate[p], speedup_vs_fp32=rate[p] / rate['fp32'],
+                       mean_ng_theta_rel_l2_vs_fp64=None if p == 'fp64' else rel_l2(r['ng'], ref['ng']),
+                       step_theta_rel_l2_vs_fp64=step_err.get(p), peak_mean_warming_k=r['peak'],
+                       injected_mw=r['injected_mw'], advected_out_mw=r['advected_out_mw'],
+                       content_rate_mw=r['content_rate_mw'], closure_residual_frac=closure,
+                       nonfinite=r['nonfinite'])
+    out = dict(metric='GLUPS (all cells) of the FP16-storage step on 600x600x64, with its 10-minute mean near-ground '
+                      'theta rel-L2 against the FP64 build', value=rate['fp16'], unit='GLUPS', n_gpus=world,
+               steps=a.steps, warmup=a.warmup, ms_per_step=N / rate['fp16'] / 1e6, higher_is_better=True,
+               scaling='weak', vs_baseline=None, dtype='f16-store/f32',
+               data='synthetic (seeded terrain and buildings; no public dataset involved)',
+               config=dict(workload=WORKLOADS['c3']['desc'], spin_steps=spin, mean_steps=mean, dt_s=dt,
+                           near_ground='first fluid cell of each column, mean over the window',
+                           parallelism=f'replicas x{world}'),
+               precision=prec, roofline=None, cpu_baseline=None, e2e=None, gpu_launches=a.steps)
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
@@ -405,13 +501,15 @@ def main():
     ap.add_argument('--block-y', type=int, default=0, help='fix the launch shape instead of autotuning')
     ap.add_argument('--zslab', type=int, default=0)
     ap.add_argument('--workload', default='c2', choices=sorted(WORKLOADS),
-                    help='c2 (the benchmark), c1 / c2q (smaller cases for profiling), c4 (64 domains in one batch), '
-                         'c5 (serving)')
+                    help='c2 (the benchmark), c1 / c2q (smaller cases for profiling), c3 (storage precision study), '
+                         'c4 (64 domains in one batch), c5 (serving)')
     ap.add_argument('--requests', type=int, default=48, help='serving: requests in the trace')
     ap.add_argument('--rate', type=float, default=50.0, help='serving: mean arrival rate (requests/s)')
     ap.add_argument('--seed', type=int, default=5, help='serving: trace seed')
     ap.add_argument('--max-cells', type=int, default=64_000_000, help='serving: resident cell budget')
     ap.add_argument('--chunk', type=int, default=64, help='serving: steps per batched chunk')
+    ap.add_argument('--spin-s', type=float, default=120.0, help='precision study: simulated spin-up seconds')
+    ap.add_argument('--mean-s', type=float, default=600.0, help='precision study: simulated averaging seconds')
     a = ap.parse_args()
     a.warmup = max(a.warmup, 3)
 
@@ -436,6 +534,8 @@ def main():
         return main_batch(a, rank, world, local, dist, torch)
     if a.workload == 'c5':
         return main_serve(a, rank, world, local, dist, torch)
+    if a.workload == 'c3':
+        return main_precision(a, rank, world, local, dist, torch)
     s = make_solver(device=local, precision=a.precision, arith=a.arith, workload=a.workload)
     dev = s._dev
     nx, ny, nz = s.info['nx'], s.info['ny'], s.info['nz']
