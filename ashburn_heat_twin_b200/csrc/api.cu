@@ -269,6 +269,7 @@ ahx_status ahx_create(const ahx_dims* dims, ahx_handle** out) {
   h->dims = *dims;
   h->dims.device_ordinal = dev;
   h->esize = esize;
+  h->esize_g = element_bytes_g(dims->precision);
   h->px = px;
   h->ps = (uint32_t)ps;
   h->qs = (uint32_t)qs;
@@ -288,7 +289,7 @@ ahx_status ahx_create(const ahx_dims* dims, ahx_handle** out) {
   if (cudaStreamCreateWithFlags(&h->s_step, cudaStreamNonBlocking) != cudaSuccess ||
       cudaStreamCreateWithFlags(&h->s_copy, cudaStreamNonBlocking) != cudaSuccess)
     return bail(AHX_EDEVICE, "live solver: stream creation failed");
-  const size_t fbytes = 19 * qs * esize, gbytes = 7 * qs * esize;
+  const size_t fbytes = 19 * qs * esize, gbytes = 7 * qs * (size_t)element_bytes_g(dims->precision);
   const size_t NXY = (size_t)dims->nx * dims->ny;
   for (int p = 0; p < 2; ++p) {
     if (cudaMalloc(&h->f[p], fbytes) != cudaSuccess || cudaMalloc(&h->g[p], gbytes) != cudaSuccess)
@@ -304,8 +305,8 @@ ahx_status ahx_create(const ahx_dims* dims, ahx_handle** out) {
       cudaMalloc(&h->d_err, sizeof(int)) != cudaSuccess)
     return bail(AHX_ENOMEM, "live solver: buffer allocation failed (out of memory)");
   cudaMemsetAsync(h->d_err, 0, sizeof(int), h->s_step);
-  h->maps_ok = true;
-  for (int t = 0; t < 2; ++t)
+  h->maps_ok = h->esize == h->esize_g;   // the staged kernel stages f and g with one element size
+  for (int t = 0; t < 2 && h->maps_ok; ++t)
     for (int p = 0; p < 2; ++p) h->maps_ok = h->maps_ok && make_maps(h, h->f[p], h->g[p], t ? 8 : 4, &h->maps[t][p]);
   cudaMemsetAsync(h->d_params, 0, 64 + 16 * (size_t)dims->nz, h->s_step);
   cudaMemsetAsync(h->d_colv, 0, NXY * sizeof(uint4), h->s_step);
@@ -355,8 +356,8 @@ ahx_status ahx_get_info(ahx_handle* h, ahx_info_out* out) {
   out->parity = h->parity;
   out->device_ordinal = h->dev;
   out->steps = h->steps;
-  out->state_bytes = 2ull * 26ull * h->qs * h->esize;
-  out->bytes_per_cell = 2ull * 26ull * h->esize;
+  out->state_bytes = 2ull * h->qs * (19ull * h->esize + 7ull * h->esize_g);
+  out->bytes_per_cell = 2ull * (19ull * h->esize + 7ull * h->esize_g);
   std::snprintf(out->device_name, sizeof(out->device_name), "%s", h->name);
   if (h->destroyed) return fail(AHX_EDESTROYED, "live solver: destroyed");
   return AHX_OK;
@@ -417,7 +418,7 @@ ahx_status ahx_clear_heat(ahx_handle* h) {
   std::lock_guard<std::mutex> lk(h->mu);
   if (ahx_status st = check(h)) return st;
   AHX_CUDA(h, cudaSetDevice(h->dev));
-  for (int p = 0; p < 2; ++p) AHX_CUDA(h, cudaMemsetAsync(h->g[p], 0, 7ull * h->qs * h->esize, h->s_step));
+  for (int p = 0; p < 2; ++p) AHX_CUDA(h, cudaMemsetAsync(h->g[p], 0, 7ull * h->qs * h->esize_g, h->s_step));
   return AHX_OK;
 }
 
@@ -796,7 +797,7 @@ ahx_status ahx_autotune(ahx_handle* h, int steps_per_trial, int* best_block_y, i
   if (steps_per_trial < 1) steps_per_trial = 4;
   AHX_CUDA(h, cudaSetDevice(h->dev));
   // trials ping-pong between the two state buffers, so they would advance the state: run them on a copy
-  const size_t fbytes = 19ull * h->qs * h->esize, gbytes = 7ull * h->qs * h->esize;
+  const size_t fbytes = 19ull * h->qs * h->esize, gbytes = 7ull * h->qs * h->esize_g;
   void *f0 = nullptr, *f1 = nullptr, *g0 = nullptr, *g1 = nullptr;
   if (cudaMalloc(&f0, fbytes) != cudaSuccess || cudaMalloc(&f1, fbytes) != cudaSuccess ||
       cudaMalloc(&g0, gbytes) != cudaSuccess || cudaMalloc(&g1, gbytes) != cudaSuccess) {

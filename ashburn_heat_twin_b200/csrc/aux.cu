@@ -13,9 +13,13 @@ int element_bytes(int precision) {
     case 1: return 2;
     case 2: return 2;
     case 3: return 8;
+    case 4: return 2;   // f FP16, g f32
+    case 5: return 2;   // f BF16, g f32
     default: return 0;
   }
 }
+
+int element_bytes_g(int precision) { return precision == 4 || precision == 5 ? 4 : element_bytes(precision); }
 
 namespace {
 
@@ -31,7 +35,7 @@ __device__ __forceinline__ void load_params_smem(const DomainView& D, ParamsHead
 // every column, north-up [row][col]; zeros where ktop >= nz.
 template <class S>
 __global__ void __launch_bounds__(128) surf_kernel(DomainView D, float conv, float* sout) {
-  using R = typename Codec<S>::Real;
+  using R = RealOf<S>;
   extern __shared__ float4 prof[];
   __shared__ ParamsHead sP;
   load_params_smem(D, sP, prof);
@@ -66,8 +70,9 @@ __global__ void __launch_bounds__(128) surf_kernel(DomainView D, float conv, flo
 template <class S>
 __global__ void __launch_bounds__(256) vol_kernel(DomainView D, int nzv, float volscale, uint32_t* vout,
                                                   unsigned* tmax_bits) {
-  using R = typename Codec<S>::Real;
-  using K = Codec<S>;
+  using R = RealOf<S>;
+  using KF = CodecF<S>;
+  using KG = CodecG<S>;
   __shared__ ParamsHead sP;
   __shared__ unsigned wmax;
   const int tid = threadIdx.x;
@@ -79,7 +84,7 @@ __global__ void __launch_bounds__(256) vol_kernel(DomainView D, int nzv, float v
   const long NVOL = (long)nzv * NXY;
   const long NW = (NVOL + 3) / 4;
   const long t = (long)blockIdx.x * blockDim.x + tid;
-  const S* gA = static_cast<const S*>(D.gA);
+  const StoreG<S>* gA = static_cast<const StoreG<S>*>(D.gA);
   float tmax = 0.f;
   if (t < NW) {
     uint32_t packed = 0;
@@ -96,27 +101,27 @@ __global__ void __launch_bounds__(256) vol_kernel(DomainView D, int nzv, float v
         if (k >= kg) {
           const uint32_t n = (uint32_t)k * D.ps + (uint32_t)j * (uint32_t)D.px + (uint32_t)i;
           R g[7];
-          g[0] = K::dec_g(K::load(gA + n));
+          g[0] = KG::dec_g(KG::load(gA + n));
           static_for<6>([&](auto Qm1) {
             constexpr int q = Qm1 + 1;
             constexpr int cx = kC7[q][0], cy = kC7[q][1], cz = kC7[q][2];
             const int si = i - cx, sj = j - cy, sk = k - cz;
             R gv;
             if (sk >= nz) {
-              gv = K::dec_g(K::load(gA + (uint32_t)q * D.qs + n));
+              gv = KG::dec_g(KG::load(gA + (uint32_t)q * D.qs + n));
             } else if (si < 0 || si >= nx || sj < 0 || sj >= ny) {
               bool inflow = false;
               if constexpr (cx == 1) inflow = inflow || (si < 0 && sP.inflow_w != 0);
               if constexpr (cx == -1) inflow = inflow || (si >= nx && sP.inflow_e != 0);
               if constexpr (cy == 1) inflow = inflow || (sj < 0 && sP.inflow_s != 0);
               if constexpr (cy == -1) inflow = inflow || (sj >= ny && sP.inflow_n != 0);
-              gv = inflow ? R(0) : K::dec_g(K::load(gA + (uint32_t)q * D.qs + n));
+              gv = inflow ? R(0) : KG::dec_g(KG::load(gA + (uint32_t)q * D.qs + n));
             } else if (sk < (int)__ldg(D.ktop + (long)sj * nx + si)) {
-              gv = K::dec_g(K::load(gA + (uint32_t)opp7(q) * D.qs + n));
+              gv = KG::dec_g(KG::load(gA + (uint32_t)opp7(q) * D.qs + n));
             } else {
               // the offset wraps in 32 bits before it touches the pointer (cx = -1 gives a negative shift)
               const uint32_t off = (uint32_t)q * D.qs + n - (uint32_t)(cx + cy * D.px + cz * (int)D.ps);
-              gv = K::dec_g(K::load(gA + off));
+              gv = KG::dec_g(KG::load(gA + off));
             }
             g[q] = gv;
           });
@@ -145,9 +150,10 @@ __global__ void __launch_bounds__(256) vol_kernel(DomainView D, int nzv, float v
 // genInitWGSL (kernel.js:524-553): equilibrium with the inflow profile at the local height above terrain in every
 // cell (solid ones included), written to both population buffers.
 template <class S>
-__global__ void __launch_bounds__(256) init_kernel(DomainView D, S* f0, S* f1) {
-  using R = typename Codec<S>::Real;
-  using K = Codec<S>;
+__global__ void __launch_bounds__(256) init_kernel(DomainView D, StoreF<S>* f0, StoreF<S>* f1) {
+  using R = RealOf<S>;
+  using KF = CodecF<S>;
+  using KG = CodecG<S>;
   const float4* prof = reinterpret_cast<const float4*>(D.params + 64);
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y;
@@ -163,7 +169,7 @@ __global__ void __launch_bounds__(256) init_kernel(DomainView D, S* f0, S* f1) {
     constexpr int q = Q;
     const R cu = R(kC19[q][0]) * U + R(kC19[q][1]) * V;
     const R fq = R(w19(q)) * (R(1.0) + R(3.0) * cu + R(4.5) * cu * cu - R(1.5) * usq);
-    const S e = K::enc_f(fq, R(w19(q)));
+    const StoreF<S> e = KF::enc_f(fq, R(w19(q)));
     f0[(uint32_t)q * D.qs + n] = e;
     f1[(uint32_t)q * D.qs + n] = e;
   });
@@ -172,9 +178,11 @@ __global__ void __launch_bounds__(256) init_kernel(DomainView D, S* f0, S* f1) {
 // genReinitWGSL (kernel.js:557-575): cells that turned from solid to fluid (k in [ktop, min(oldk, nz))) get rest
 // equilibrium f = w and theta = 0.
 template <class S>
-__global__ void __launch_bounds__(256) reinit_kernel(DomainView D, const uint32_t* oldk, S* f, S* g) {
-  using R = typename Codec<S>::Real;
-  using K = Codec<S>;
+__global__ void __launch_bounds__(256) reinit_kernel(DomainView D, const uint32_t* oldk, StoreF<S>* f,
+                                                      StoreG<S>* g) {
+  using R = RealOf<S>;
+  using KF = CodecF<S>;
+  using KG = CodecG<S>;
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   const int NXY = D.nx * D.ny;
   if (c >= NXY) return;
@@ -184,11 +192,11 @@ __global__ void __launch_bounds__(256) reinit_kernel(DomainView D, const uint32_
     const uint32_t n = (uint32_t)k * D.ps + (uint32_t)j * (uint32_t)D.px + (uint32_t)i;
     static_for<19>([&](auto Q) {
       constexpr int q = Q;
-      f[(uint32_t)q * D.qs + n] = K::enc_f(R(w19(q)), R(w19(q)));
+      f[(uint32_t)q * D.qs + n] = KF::enc_f(R(w19(q)), R(w19(q)));
     });
     static_for<7>([&](auto Q) {
       constexpr int q = Q;
-      g[(uint32_t)q * D.qs + n] = K::enc_g(R(0));
+      g[(uint32_t)q * D.qs + n] = KG::enc_g(R(0));
     });
   }
 }
@@ -197,10 +205,11 @@ __global__ void __launch_bounds__(256) reinit_kernel(DomainView D, const uint32_
 // 0.5|j|^2/rho, rho - 1, 1) summed in FP64, max theta (>= 0), non-finite count (rho or theta), max |j|/rho.
 template <class S>
 __global__ void __launch_bounds__(256) stats_kernel(DomainView D, StatsScratch* out) {
-  using R = typename Codec<S>::Real;
-  using K = Codec<S>;
-  const S* fA = static_cast<const S*>(D.fA);
-  const S* gA = static_cast<const S*>(D.gA);
+  using R = RealOf<S>;
+  using KF = CodecF<S>;
+  using KG = CodecG<S>;
+  const StoreF<S>* fA = static_cast<const StoreF<S>*>(D.fA);
+  const StoreG<S>* gA = static_cast<const StoreG<S>*>(D.gA);
   const int nx = D.nx, ny = D.ny, nz = D.nz;
   const long total = (long)nx * ny * nz;
   double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
@@ -215,16 +224,16 @@ __global__ void __launch_bounds__(256) stats_kernel(DomainView D, StatsScratch* 
     R f[19];
     static_for<19>([&](auto Q) {
       constexpr int q = Q;
-      f[q] = K::dec_f(K::load(fA + (uint32_t)q * D.qs + n), R(w19(q)));
+      f[q] = KF::dec_f(KF::load(fA + (uint32_t)q * D.qs + n), R(w19(q)));
     });
     float rho = (float)f[0];
 #pragma unroll
     for (int q = 1; q < 19; ++q) rho = rho + (float)f[q];
     auto fq = [&](int q) { return (float)f[q]; };
     const float jx = moment1<float, 0>(fq), jy = moment1<float, 1>(fq), jz = moment1<float, 2>(fq);
-    float th = (float)K::dec_g(K::load(gA + n));
+    float th = (float)KG::dec_g(KG::load(gA + n));
 #pragma unroll
-    for (int q = 1; q < 7; ++q) th = th + (float)K::dec_g(K::load(gA + (uint32_t)q * D.qs + n));
+    for (int q = 1; q < 7; ++q) th = th + (float)KG::dec_g(KG::load(gA + (uint32_t)q * D.qs + n));
     const unsigned br = __float_as_uint(rho) & 0x7f800000u, bt = __float_as_uint(th) & 0x7f800000u;
     if (br == 0x7f800000u || bt == 0x7f800000u) {
       ++nonf;
@@ -261,11 +270,11 @@ __global__ void __launch_bounds__(256) stats_kernel(DomainView D, StatsScratch* 
 }
 
 // reference plane [cell] (f32 or f64) <-> internal pitched plane q
-template <class S>
-__global__ void __launch_bounds__(256) import_plane_kernel(DomainView D, const void* ref, int ref_is_f64, S* dst,
+template <class T>
+__global__ void __launch_bounds__(256) import_plane_kernel(DomainView D, const void* ref, int ref_is_f64, T* dst,
                                                            int q, int is_g) {
-  using R = typename Codec<S>::Real;
-  using K = Codec<S>;
+  using R = typename Codec<T>::Real;
+  using K = Codec<T>;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y, k = blockIdx.z;
   if (i >= D.nx) return;
@@ -276,18 +285,18 @@ __global__ void __launch_bounds__(256) import_plane_kernel(DomainView D, const v
   dst[(uint32_t)q * D.qs + n] = is_g ? K::enc_g(v) : K::enc_f(v, R(w));
 }
 
-template <class S>
-__global__ void __launch_bounds__(256) export_plane_kernel(DomainView D, const S* src, void* ref, int ref_is_f64,
+template <class T>
+__global__ void __launch_bounds__(256) export_plane_kernel(DomainView D, const T* src, void* ref, int ref_is_f64,
                                                            int q, int is_g) {
-  using R = typename Codec<S>::Real;
-  using K = Codec<S>;
+  using R = typename Codec<T>::Real;
+  using K = Codec<T>;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y, k = blockIdx.z;
   if (i >= D.nx) return;
   const size_t c = ((size_t)k * D.ny + j) * D.nx + i;
   const double w = q == 0 ? 1.0 / 3 : (q < 7 ? 1.0 / 18 : 1.0 / 36);
   const uint32_t n = (uint32_t)k * D.ps + (uint32_t)j * (uint32_t)D.px + (uint32_t)i;
-  const S e = src[(uint32_t)q * D.qs + n];
+  const T e = src[(uint32_t)q * D.qs + n];
   const R v = is_g ? K::dec_g(e) : K::dec_f(e, R(w));
   if (ref_is_f64) static_cast<double*>(ref)[c] = (double)v;
   else static_cast<float*>(ref)[c] = (float)v;
@@ -300,6 +309,8 @@ cudaError_t dispatch(int precision, F&& f) {
     case 1: return f(__half{});
     case 2: return f(__nv_bfloat16{});
     case 3: return f(double{});
+    case 4: return f(Mixed<__half, float>{});
+    case 5: return f(Mixed<__nv_bfloat16, float>{});
     default: return cudaErrorInvalidValue;
   }
 }
@@ -310,7 +321,7 @@ cudaError_t launch_init(const DomainView& D, int precision, void* f0, void* f1, 
   return dispatch(precision, [&](auto tag) {
     using S = decltype(tag);
     dim3 grid((D.nx + 255) / 256, D.ny, D.nz);
-    init_kernel<S><<<grid, 256, 0, s>>>(D, static_cast<S*>(f0), static_cast<S*>(f1));
+    init_kernel<S><<<grid, 256, 0, s>>>(D, static_cast<StoreF<S>*>(f0), static_cast<StoreF<S>*>(f1));
     return cudaGetLastError();
   });
 }
@@ -320,7 +331,8 @@ cudaError_t launch_reinit(const DomainView& D, int precision, const uint32_t* ol
   return dispatch(precision, [&](auto tag) {
     using S = decltype(tag);
     const int NXY = D.nx * D.ny;
-    reinit_kernel<S><<<(NXY + 255) / 256, 256, 0, s>>>(D, oldk, static_cast<S*>(f), static_cast<S*>(g));
+    reinit_kernel<S><<<(NXY + 255) / 256, 256, 0, s>>>(D, oldk, static_cast<StoreF<S>*>(f),
+                                                       static_cast<StoreG<S>*>(g));
     return cudaGetLastError();
   });
 }
@@ -361,7 +373,10 @@ cudaError_t launch_import_plane(const DomainView& D, int precision, const void* 
   return dispatch(precision, [&](auto tag) {
     using S = decltype(tag);
     dim3 grid((D.nx + 255) / 256, D.ny, D.nz);
-    import_plane_kernel<S><<<grid, 256, 0, s>>>(D, ref_plane, ref_is_f64, static_cast<S*>(dst), q, is_g);
+    if (is_g)
+      import_plane_kernel<StoreG<S>><<<grid, 256, 0, s>>>(D, ref_plane, ref_is_f64, static_cast<StoreG<S>*>(dst), q, 1);
+    else
+      import_plane_kernel<StoreF<S>><<<grid, 256, 0, s>>>(D, ref_plane, ref_is_f64, static_cast<StoreF<S>*>(dst), q, 0);
     return cudaGetLastError();
   });
 }
@@ -371,7 +386,12 @@ cudaError_t launch_export_plane(const DomainView& D, int precision, const void* 
   return dispatch(precision, [&](auto tag) {
     using S = decltype(tag);
     dim3 grid((D.nx + 255) / 256, D.ny, D.nz);
-    export_plane_kernel<S><<<grid, 256, 0, s>>>(D, static_cast<const S*>(src), ref_plane, ref_is_f64, q, is_g);
+    if (is_g)
+      export_plane_kernel<StoreG<S>><<<grid, 256, 0, s>>>(D, static_cast<const StoreG<S>*>(src), ref_plane,
+                                                          ref_is_f64, q, 1);
+    else
+      export_plane_kernel<StoreF<S>><<<grid, 256, 0, s>>>(D, static_cast<const StoreF<S>*>(src), ref_plane,
+                                                          ref_is_f64, q, 0);
     return cudaGetLastError();
   });
 }

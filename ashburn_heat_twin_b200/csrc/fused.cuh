@@ -160,12 +160,13 @@ struct Cell {
 // secProfile + secOutflowPrelude + secStreamF + secStreamG for cell (C.i, C.j, k); n is the pitched cell index.
 template <class S>
 __device__ __forceinline__ void stream_cell(const DomainView& D, const ParamsHead& P, const float4* prof,
-                                            const Column<typename Codec<S>::Real>& C, int k, uint32_t n,
-                                            Cell<typename Codec<S>::Real>& X) {
-  using R = typename Codec<S>::Real;
-  using K = Codec<S>;
-  const S* fA = static_cast<const S*>(D.fA);
-  const S* gA = static_cast<const S*>(D.gA);
+                                            const Column<RealOf<S>>& C, int k, uint32_t n,
+                                            Cell<RealOf<S>>& X) {
+  using R = RealOf<S>;
+  using KF = CodecF<S>;
+  using KG = CodecG<S>;
+  const StoreF<S>* fA = static_cast<const StoreF<S>*>(D.fA);
+  const StoreG<S>* gA = static_cast<const StoreG<S>*>(D.gA);
   const uint32_t qs = D.qs, ps = D.ps, px = (uint32_t)D.px;
   const bool top = (k == D.nz - 1);
   // secProfile
@@ -179,7 +180,7 @@ __device__ __forceinline__ void stream_cell(const DomainView& D, const ParamsHea
   X.kb = R(pr.z);
 
   // secStreamF / secStreamG as an index remap: one load per population
-  X.f[0] = K::dec_f(K::load(fA + n), R(w19(0)));
+  X.f[0] = KF::dec_f(KF::load(fA + n), R(w19(0)));
   static_for<18>([&](auto Qm1) {
     constexpr int q = Qm1 + 1;
     constexpr int cx = kC19[q][0], cy = kC19[q][1], cz = kC19[q][2];
@@ -199,9 +200,9 @@ __device__ __forceinline__ void stream_cell(const DomainView& D, const ParamsHea
     } else {
       off = (uint32_t)q * qs + n - (uint32_t)(cx + cy * (int)px + cz * (int)ps);
     }
-    X.f[q] = K::dec_f(K::load(fA + off), R(w19(q)));
+    X.f[q] = KF::dec_f(KF::load(fA + off), R(w19(q)));
   });
-  X.g[0] = K::dec_g(K::load(gA + n));
+  X.g[0] = KG::dec_g(KG::load(gA + n));
   static_for<6>([&](auto Qm1) {
     constexpr int q = Qm1 + 1;
     constexpr int cx = kC7[q][0], cy = kC7[q][1], cz = kC7[q][2];
@@ -215,7 +216,7 @@ __device__ __forceinline__ void stream_cell(const DomainView& D, const ParamsHea
     } else {
       off = (uint32_t)q * qs + n - (uint32_t)(cx + cy * (int)px + cz * (int)ps);
     }
-    X.g[q] = K::dec_g(K::load(gA + off));
+    X.g[q] = KG::dec_g(KG::load(gA + off));
   });
 
   if (C.face) {
@@ -225,7 +226,7 @@ __device__ __forceinline__ void stream_cell(const DomainView& D, const ParamsHea
       R own[19];
       static_for<19>([&](auto Q) {
         constexpr int q = Q;
-        own[q] = K::dec_f(K::load(fA + (uint32_t)q * qs + n), R(w19(q)));
+        own[q] = KF::dec_f(KF::load(fA + (uint32_t)q * qs + n), R(w19(q)));
       });
       rn = own[0];
 #pragma unroll
@@ -280,12 +281,13 @@ __device__ __forceinline__ void stream_cell(const DomainView& D, const ParamsHea
 // per population at a fixed offset; loads exactly the values stream_cell would.
 template <class S>
 __device__ __forceinline__ void stream_interior(const DomainView& D, const float4* prof,
-                                                const Column<typename Codec<S>::Real>& C, int k, uint32_t n,
-                                                Cell<typename Codec<S>::Real>& X) {
-  using R = typename Codec<S>::Real;
-  using K = Codec<S>;
-  const S* fA = static_cast<const S*>(D.fA);
-  const S* gA = static_cast<const S*>(D.gA);
+                                                const Column<RealOf<S>>& C, int k, uint32_t n,
+                                                Cell<RealOf<S>>& X) {
+  using R = RealOf<S>;
+  using KF = CodecF<S>;
+  using KG = CodecG<S>;
+  const StoreF<S>* fA = static_cast<const StoreF<S>*>(D.fA);
+  const StoreG<S>* gA = static_cast<const StoreG<S>*>(D.gA);
   int zagl = k - C.ktc;
   if (zagl < 0) zagl = 0;
   if (zagl > D.nz - 1) zagl = D.nz - 1;
@@ -295,11 +297,11 @@ __device__ __forceinline__ void stream_interior(const DomainView& D, const float
   X.kb = R(pr.z);
   static_for<19>([&](auto Q) {
     constexpr int q = Q;
-    X.f[q] = K::dec_f(K::load(fA + (n + D.pull_f[q])), R(w19(q)));
+    X.f[q] = KF::dec_f(KF::load(fA + (n + D.pull_f[q])), R(w19(q)));
   });
   static_for<7>([&](auto Q) {
     constexpr int q = Q;
-    X.g[q] = K::dec_g(K::load(gA + (n + D.pull_g[q])));
+    X.g[q] = KG::dec_g(KG::load(gA + (n + D.pull_g[q])));
   });
 }
 
@@ -362,13 +364,14 @@ __device__ __forceinline__ void moments_forces(const ParamsHead& P, const Column
 // secRelax + secCollision + secScalarCollision (kernel.js:308-386); writes the next state of cell n
 template <class S>
 __device__ __forceinline__ void collide_store(const DomainView& D, const ParamsHead& P,
-                                              const Column<typename Codec<S>::Real>& C, int k, uint32_t n,
-                                              const Cell<typename Codec<S>::Real>& X,
-                                              const Macro<typename Codec<S>::Real>& M) {
-  using R = typename Codec<S>::Real;
-  using K = Codec<S>;
-  S* fB = static_cast<S*>(D.fB);
-  S* gB = static_cast<S*>(D.gB);
+                                              const Column<RealOf<S>>& C, int k, uint32_t n,
+                                              const Cell<RealOf<S>>& X,
+                                              const Macro<RealOf<S>>& M) {
+  using R = RealOf<S>;
+  using KF = CodecF<S>;
+  using KG = CodecG<S>;
+  StoreF<S>* fB = static_cast<StoreF<S>*>(D.fB);
+  StoreG<S>* gB = static_cast<StoreG<S>*>(D.gB);
   const uint32_t qs = D.qs;
   const R rho = M.rho, ux = M.ux, uy = M.uy, uz = M.uz, Fx = M.Fx, Fy = M.Fy, Fz = M.Fz;
   const R* f = X.f;
@@ -416,7 +419,7 @@ __device__ __forceinline__ void collide_store(const DomainView& D, const ParamsH
     const R fr = w45 * (qn - trN);
     const R cF = cdot<R, cx, cy, cz>(Fx, Fy, Fz);
     const R Fq = fpre * w * (R(3.0) * (cF - uF) + R(9.0) * cu * cF);
-    K::store(fB + (n + D.plane[q]), K::enc_f(feq + om * fr + Fq, w));
+    KF::store(fB + (n + D.plane[q]), KF::enc_f(feq + om * fr + Fq, w));
   });
   R Ssrc = R(0);
   if (k == C.kg) Ssrc = R(C.qsrc) * R(P.srcscale);
@@ -426,7 +429,7 @@ __device__ __forceinline__ void collide_store(const DomainView& D, const ParamsH
     constexpr int cx = kC7[q][0], cy = kC7[q][1], cz = kC7[q][2];
     const R w = R(w7(q));
     const R geq = w * M.th * (R(1.0) + R(4.0) * cdot<R, cx, cy, cz>(ux, uy, uz));
-    K::store(gB + (n + D.plane[q]), K::enc_g((X.g[q] + omg * (geq - X.g[q]) + w * Ssrc) * (R(1.0) - M.sg)));
+    KG::store(gB + (n + D.plane[q]), KG::enc_g((X.g[q] + omg * (geq - X.g[q]) + w * Ssrc) * (R(1.0) - M.sg)));
   });
 }
 
@@ -436,13 +439,14 @@ __device__ __forceinline__ void collide_store(const DomainView& D, const ParamsH
 // moments_forces + collide_store; rounding differs (held to the single-step theta rel-L2 <= 1e-5 bar).
 template <class S>
 __device__ __forceinline__ void fast_update(const DomainView& D, const ParamsHead& P,
-                                            const Column<typename Codec<S>::Real>& C, int k, uint32_t n,
-                                            const Cell<typename Codec<S>::Real>& X,
-                                            Macro<typename Codec<S>::Real>& M) {
-  using R = typename Codec<S>::Real;
-  using K = Codec<S>;
-  S* fB = static_cast<S*>(D.fB);
-  S* gB = static_cast<S*>(D.gB);
+                                            const Column<RealOf<S>>& C, int k, uint32_t n,
+                                            const Cell<RealOf<S>>& X,
+                                            Macro<RealOf<S>>& M) {
+  using R = RealOf<S>;
+  using KF = CodecF<S>;
+  using KG = CodecG<S>;
+  StoreF<S>* fB = static_cast<StoreF<S>*>(D.fB);
+  StoreG<S>* gB = static_cast<StoreG<S>*>(D.gB);
   const uint32_t qs = D.qs;
   R sp9[9], dp9[9];
   static_for<9>([&](auto Pi) {
@@ -511,7 +515,7 @@ __device__ __forceinline__ void fast_update(const DomainView& D, const ParamsHea
   {
     const R w = R(w19(0));
     const R f0 = w * rho * base + om * R(4.5 * w19(0)) * (-trN) + fpre * w * (R(-3.0) * uF);
-    K::store(fB + n, K::enc_f(f0, w));
+    KF::store(fB + n, KF::enc_f(f0, w));
   }
   static_for<9>([&](auto Pi) {
     constexpr int p = Pi;
@@ -530,21 +534,21 @@ __device__ __forceinline__ void fast_update(const DomainView& D, const ParamsHea
     const R rw = rho * w, fw = fpre * w;
     const R E = rw * (base + R(4.5) * cu * cu) + om * R(4.5 * w19(q)) * (qn - trN) + fw * (R(9.0) * cu * cF - R(3.0) * uF);
     const R O = R(3.0) * (rw * cu + fw * cF);
-    K::store(fB + (n + D.plane[q]), K::enc_f(E + O, w));
-    K::store(fB + (n + D.plane[q + 1]), K::enc_f(E - O, w));
+    KF::store(fB + (n + D.plane[q]), KF::enc_f(E + O, w));
+    KF::store(fB + (n + D.plane[q + 1]), KF::enc_f(E - O, w));
   });
   const R Ssrc = (k == C.kg) ? R(C.qsrc) * R(P.srcscale) : R(0);
   const R omg = R(1.0) / taug;
   const R a = R(1.0) - omg, one_sg = R(1.0) - sg;
-  K::store(gB + n, K::enc_g((a * X.g[0] + omg * R(w7(0)) * th + R(w7(0)) * Ssrc) * one_sg));
+  KG::store(gB + n, KG::enc_g((a * X.g[0] + omg * R(w7(0)) * th + R(w7(0)) * Ssrc) * one_sg));
   static_for<3>([&](auto Pi) {
     constexpr int p = Pi;
     constexpr int q = 2 * p + 1;
     constexpr int cx = kC7[q][0], cy = kC7[q][1], cz = kC7[q][2];
     const R b = omg * R(w7(q)) * th + R(w7(q)) * Ssrc;
     const R c4 = omg * R(4.0 * w7(q)) * th * cdot<R, cx, cy, cz>(ux, uy, uz);
-    K::store(gB + (n + D.plane[q]), K::enc_g((a * X.g[q] + b + c4) * one_sg));
-    K::store(gB + (n + D.plane[q + 1]), K::enc_g((a * X.g[q + 1] + b - c4) * one_sg));
+    KG::store(gB + (n + D.plane[q]), KG::enc_g((a * X.g[q] + b + c4) * one_sg));
+    KG::store(gB + (n + D.plane[q + 1]), KG::enc_g((a * X.g[q + 1] + b - c4) * one_sg));
   });
   M.rho = rho;
   M.jx = jx;
@@ -571,7 +575,7 @@ constexpr int kBlockX = 32;
 // The fused step over one z-slab of the columns of a block. MODE: 0 none, 1 write dbg, 2 accumulate dbg.
 template <class S, int MODE, bool BUDGET, bool FAST>
 __device__ __forceinline__ void step_block(const DomainView& D, int bx, int by, int bz, int zslab) {
-  using R = typename Codec<S>::Real;
+  using R = RealOf<S>;
   extern __shared__ float4 smem_prof[];
   __shared__ ParamsHead sP;
   const int tid = threadIdx.y * blockDim.x + threadIdx.x;

@@ -53,7 +53,7 @@ struct ahx_handle {
   std::string lost_msg;
   cudaStream_t s_step = nullptr, s_copy = nullptr;
   ahx_dims dims{};
-  int esize = 4, px = 0;
+  int esize = 4, esize_g = 4, px = 0;   // bytes per stored f / g population; x pitch in elements
   uint32_t ps = 0, qs = 0;
   void* f[2] = {nullptr, nullptr};
   void* g[2] = {nullptr, nullptr};

@@ -129,6 +129,32 @@ struct Codec<__nv_bfloat16> {
   }
 };
 
+// Storage of a state: a plain type stores f and g alike; Mixed<SF, SG> stores the flow populations f as SF and the
+// temperature populations g as SG (16-bit f with f32 g keeps the heat budget: a per-step source increment can be
+// far below half an ulp of a 16-bit g).
+template <class SF, class SG>
+struct Mixed {};
+template <class S>
+struct StorageOf {
+  using F = S;
+  using G = S;
+};
+template <class SF, class SG>
+struct StorageOf<Mixed<SF, SG>> {
+  using F = SF;
+  using G = SG;
+};
+template <class S>
+using CodecF = Codec<typename StorageOf<S>::F>;
+template <class S>
+using CodecG = Codec<typename StorageOf<S>::G>;
+template <class S>
+using RealOf = typename CodecF<S>::Real;
+template <class S>
+using StoreF = typename StorageOf<S>::F;
+template <class S>
+using StoreG = typename StorageOf<S>::G;
+
 // Parameter block (kernel.js:44-50): 16 four-byte scalars, then nz x float4 (uin, vin, kbg, 0)
 struct ParamsHead {
   float tau0, cs2smag, gbeta, prt, kfloor, momfac, srcscale, sigmax;

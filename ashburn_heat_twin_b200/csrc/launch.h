@@ -76,7 +76,8 @@ cudaError_t launch_import_plane(const DomainView& D, int precision, const void* 
 cudaError_t launch_export_plane(const DomainView& D, int precision, const void* src, void* ref_plane, int ref_is_f64,
                                 int q, int is_g, cudaStream_t s);
 
-int element_bytes(int precision);
+int element_bytes(int precision);     // bytes of one stored flow population f
+int element_bytes_g(int precision);   // bytes of one stored temperature population g
 
 // the thread-local message ahx_last_error() returns (api.cu)
 void set_last_error(const std::string& m);

@@ -3,6 +3,8 @@
 // -fmad=false and -fmad=true respectively.
 #pragma once
 
+#include <type_traits>
+
 #include "fused.cuh"
 #include "launch.h"
 #include "tma.cuh"
@@ -89,6 +91,8 @@ cudaError_t launch_batch(const BatchLaunch& B, cudaStream_t s, int* occupancy) {
     case 1: return batch_s<__half>(B, s, occupancy);
     case 2: return batch_s<__nv_bfloat16>(B, s, occupancy);
     case 3: return batch_s<double>(B, s, occupancy);
+    case 4: return batch_s<Mixed<__half, float>>(B, s, occupancy);
+    case 5: return batch_s<Mixed<__nv_bfloat16, float>>(B, s, occupancy);
     default: return cudaErrorInvalidValue;
   }
 }
@@ -128,7 +132,8 @@ static cudaError_t launch_tma(const DomainView& D, const StepLaunch& L, cudaStre
 
 template <class S, int MODE, bool BUDGET>
 static cudaError_t launch_t(const DomainView& D, const StepLaunch& L, cudaStream_t s) {
-  if constexpr (MODE == 0 && !BUDGET) {
+  if constexpr (MODE == 0 && !BUDGET && std::is_same_v<StoreF<S>, StoreG<S>>) {
+    // the staged kernel stages f and g with one element size: uniform storages only
     if (L.tma_ty > 0 && L.maps != nullptr) return launch_tma<S>(D, L, s);
   }
   const int minb = (MODE == 0 && !BUDGET) ? L.minb : 0;
@@ -177,6 +182,8 @@ cudaError_t launch_step(const DomainView& D, const StepLaunch& L, cudaStream_t s
     case 1: return launch_s<__half>(D, L, s);
     case 2: return launch_s<__nv_bfloat16>(D, L, s);
     case 3: return launch_s<double>(D, L, s);
+    case 4: return launch_s<Mixed<__half, float>>(D, L, s);
+    case 5: return launch_s<Mixed<__nv_bfloat16, float>>(D, L, s);
     default: return cudaErrorInvalidValue;
   }
 }

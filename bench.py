@@ -48,6 +48,10 @@ WORKLOADS = {
                     'wind, roof flux and one 120 MW campus per request, synthetic seed 1 box', spec='C1'),
 }
 METRIC = 'GLUPS (all cells) of the fused D3Q19+D3Q7 step, 600x600x64'
+# algorithmic bytes per fluid-cell update: read + write of 19 f and 7 g populations at their storage widths
+CELL_BYTES = {'fp32': 208, 'fp16': 104, 'bf16': 104, 'fp64': 416, 'fp16g32': 132, 'bf16g32': 132}
+DTYPE = {'fp32': 'f32', 'fp16': 'f16-store/f32', 'bf16': 'bf16-store/f32', 'fp64': 'f64',
+         'fp16g32': 'f16-store f, f32-store g / f32', 'bf16g32': 'bf16-store f, f32-store g / f32'}
 
 
 def log(*a):
@@ -242,8 +246,7 @@ def main_batch(a, rank, world, local, dist, torch):
     value = world * cells * a.steps / (ms_all / 1e3) / 1e9
     # the same members stepped one after another with their own tuned launches (no batch)
     serial_ms = sum(s._dev.time_steps(a.steps) for s in solvers)
-    esize = {'fp32': 4, 'fp16': 2, 'bf16': 2, 'fp64': 8}[a.precision]
-    bytes_launch = fluid * 52 * esize
+    bytes_launch = fluid * CELL_BYTES[a.precision]
     launch_ms = ms / a.steps
     achieved = bytes_launch / (launch_ms / 1e3) / 1e9
     peak, peak_kind = measured_peaks()
@@ -285,11 +288,11 @@ def main_batch(a, rank, world, local, dist, torch):
     out = dict(metric='GLUPS (all cells) of the batched fused D3Q19+D3Q7 step, 64 domains (32 x 200x200x32 + '
                       '32 x 150x150x24)', value=value, unit='GLUPS', n_gpus=world, steps=a.steps, warmup=a.warmup,
                ms_per_step=ms_all / a.steps, higher_is_better=True, scaling='weak', vs_baseline=None,
-               dtype={'fp32': 'f32', 'fp16': 'f16-store/f32', 'bf16': 'bf16-store/f32', 'fp64': 'f64'}[a.precision],
+               dtype=DTYPE[a.precision],
                data='synthetic (seeded terrain, buildings and scenarios; no public dataset involved)',
                config=dict(workload=WORKLOADS['c4']['desc'], precision=a.precision, arith=a.arith, scheme='pull',
                            parallelism=f'replicas x{world}', cells=cells, fluid_cells=fluid,
-                           l2=f'state {cells * 52 * esize / 1e9:.1f} GB vs 126 MB L2', tuned=tuned,
+                           l2=f'state {cells * CELL_BYTES[a.precision] / 1e9:.1f} GB vs 126 MB L2', tuned=tuned,
                            batch=dict(tiles=info['tiles'], grid=info['grid'], minb=info['minb'],
                                       zslab_max=info['zslab_max'], graph=bool(info['use_graph']), tuned=btune)),
                serial=dict(value=world * cells * a.steps / (serial_ms / 1e3) / 1e9, unit='GLUPS',
@@ -368,7 +371,7 @@ def main_serve(a, rank, world, local, dist, torch):
                value=stats['glups'], unit='GLUPS', n_gpus=world, steps=stats['batch_steps'], warmup=6,
                ms_per_step=stats['makespan_s'] * 1e3 / max(1, stats['batch_steps']), higher_is_better=True,
                scaling='weak', vs_baseline=None,
-               dtype={'fp32': 'f32', 'fp16': 'f16-store/f32', 'bf16': 'bf16-store/f32', 'fp64': 'f64'}[a.precision],
+               dtype=DTYPE[a.precision],
                data='synthetic (seeded terrain, buildings and request trace; no public dataset involved)',
                config=dict(workload=WORKLOADS['c5']['desc'], requests=a.requests, rate_hz=a.rate, seed=a.seed,
                            precision=a.precision, arith=a.arith, max_cells=a.max_cells, chunk=a.chunk,
@@ -403,7 +406,7 @@ def main_precision(a, rank, world, local, dist, torch):
     import numpy as np
 
     from ashburn_heat_twin_b200 import params as PM
-    order = ['fp64', 'fp32', 'fp16', 'bf16']
+    order = ['fp64', 'fp32', 'fp16', 'bf16', 'fp16g32', 'bf16g32']
     sol = {p: make_solver(device=local, precision=p, arith='exact' if p == 'fp64' else 'fast') for p in order}
     s0 = sol['fp64']
     nx, ny, nz = s0.info['nx'], s0.info['ny'], s0.info['nz']
@@ -493,7 +496,7 @@ def main():
     ap.add_argument('--steps', type=int, default=20)
     ap.add_argument('--warmup', type=int, default=5)
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
-    ap.add_argument('--precision', default='fp32', choices=['fp32', 'fp16', 'bf16', 'fp64'])
+    ap.add_argument('--precision', default='fp32', choices=sorted(CELL_BYTES))
     ap.add_argument('--arith', default='fast', choices=['exact', 'fast'])
     ap.add_argument('--frame', type=int, default=10, help='steps per e2e frame (setMet + step(F) + read())')
     ap.add_argument('--no-cpu-baseline', action='store_true')
@@ -570,8 +573,7 @@ def main():
 
     # roofline of the step kernel (one launch per step): algorithmic bytes = fluid cells x (read + write of 19 f and
     # 7 g populations) at the storage width
-    esize = {'fp32': 4, 'fp16': 2, 'bf16': 2, 'fp64': 8}[a.precision]
-    bytes_launch = fluid * 52 * esize
+    bytes_launch = fluid * CELL_BYTES[a.precision]
     launch_ms = ms / a.steps
     achieved = bytes_launch / (launch_ms / 1e3) / 1e9
     peak, peak_kind = measured_peaks()
@@ -619,7 +621,7 @@ def main():
     metric = METRIC.replace('600x600x64', WORKLOADS[a.workload]['desc'].split(' cells')[0])
     out = dict(metric=metric, value=value, unit='GLUPS', n_gpus=world, steps=a.steps, warmup=a.warmup,
                ms_per_step=ms_all / a.steps, higher_is_better=True, scaling='weak', vs_baseline=None,
-               dtype={'fp32': 'f32', 'fp16': 'f16-store/f32', 'bf16': 'bf16-store/f32', 'fp64': 'f64'}[a.precision],
+               dtype=DTYPE[a.precision],
                data='synthetic (seeded terrain and buildings; no public dataset involved)',
                config=dict(workload=WORKLOADS[a.workload]['desc'], precision=a.precision, arith=a.arith, scheme='pull',
                            parallelism=f'replicas x{world}', fluid_cells=fluid, l2=f"state {s._dev.info()['state_bytes'] / 1e9:.2f} GB vs 126 MB L2",

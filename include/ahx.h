@@ -37,7 +37,17 @@ typedef enum {
   AHX_EBUSY = 7        /* no free read slot (more than AHX_MAX_READS reads in flight) */
 } ahx_status;
 
-typedef enum { AHX_FP32 = 0, AHX_FP16 = 1, AHX_BF16 = 2, AHX_FP64 = 3 } ahx_precision;
+/* storage of the populations (arithmetic is f32, f64 for AHX_FP64). The 16-bit formats store (f - w) * scale for the
+ * flow populations; AHX_FP16_G32 / AHX_BF16_G32 store f in 16 bits and the temperature populations g in f32, which
+ * keeps the heat budget (a per-step source increment can be far below half an ulp of a 16-bit g). */
+typedef enum {
+  AHX_FP32 = 0,
+  AHX_FP16 = 1,
+  AHX_BF16 = 2,
+  AHX_FP64 = 3,
+  AHX_FP16_G32 = 4,
+  AHX_BF16_G32 = 5
+} ahx_precision;
 
 /* step output modes (kernel.js:427-428; solver.js:551-558 stepOut / stepAcc) */
 typedef enum { AHX_MODE_NONE = 0, AHX_MODE_OUT = 1, AHX_MODE_ACC = 2 } ahx_mode;

@@ -143,10 +143,10 @@ def test_fp64_build_bit_exact_with_fp64_oracle():
     o.destroy()
 
 
-@pytest.mark.parametrize('precision,tol', [('fp16', 2e-3), ('bf16', 2e-2)])
+@pytest.mark.parametrize('precision,tol', [('fp16', 2e-3), ('bf16', 2e-2), ('fp16g32', 2e-3), ('bf16g32', 2e-2)])
 def test_16bit_storage_error_vs_fp64(precision, tol):
-    """16-bit population storage (shifted by w_q, scaled) against the FP64 build after 300 steps with heat on:
-    theta rel-L2 over fluid cells within the stated tolerance."""
+    """16-bit population storage (f shifted by w_q and scaled; g likewise, or f32 for the *g32 storages) against
+    the FP64 build after 300 steps with heat on: theta rel-L2 over fluid cells within the stated tolerance."""
     met = dict(u10=5.0, dirFrom=250.0, wstar=1.5, blh=700.0)
     h = small_solver(cuda_backend(precision, 'exact'), met=met)
     d = small_solver(cuda_backend('fp64', 'exact'), met=met)
@@ -210,3 +210,18 @@ def test_launch_shapes_bit_exact(shape, zslab):
     assert np.array_equal(g._dbg.readDbg(), o._dbg.readDbg())
     g.destroy()
     o.destroy()
+
+
+def test_f32_g_storage_keeps_the_heat_content():
+    """Storing g in f32 next to 16-bit f removes the heat loss of 16-bit g: after 300 steps with heat on, the FP64
+    heat content (sum of theta) is matched far better than with FP16 g."""
+    met = dict(u10=5.0, dirFrom=250.0, wstar=1.5, blh=700.0)
+    runs = {}
+    for p in ('fp64', 'fp16', 'fp16g32'):
+        s = small_solver(cuda_backend(p, 'exact'), met=met)
+        s.step(300).result()
+        runs[p] = s._dev.stats()['sumTheta']
+        s.destroy()
+    e16 = abs(runs['fp16'] / runs['fp64'] - 1)
+    e32 = abs(runs['fp16g32'] / runs['fp64'] - 1)
+    assert e32 < e16 and e32 < 1e-4, (e16, e32)
