@@ -596,15 +596,28 @@ __device__ __forceinline__ void step_block(const DomainView& D, int bx, int by, 
 #pragma unroll
     for (int a = 0; a < 4; ++a) B.ftu[a] = B.fu[a] = 0.f;
   }
-  if (i < D.nx && j < D.ny) {
-    Column<R> C;
+  // A warp is one row of 32 columns. It walks the levels in lockstep from its lowest first fluid level, so the lanes
+  // of one load touch one level (coalesced), and it takes the interior fast path only when every active lane is
+  // interior (the general path gives identical values for interior cells, so a mixed level runs one path, not two).
+  const bool valid = i < D.nx && j < D.ny;
+  Column<R> C;
+  int kstart = k1;
+  if (valid) {
     load_column(D, P, i, j, C);
-    const uint32_t base = (uint32_t)j * (uint32_t)D.px + (uint32_t)i;
+    kstart = max(k0, C.kg);
+  }
+  const int kw = __reduce_min_sync(0xffffffffu, kstart);
+  const uint32_t base = (uint32_t)j * (uint32_t)D.px + (uint32_t)i;
 #pragma unroll 1
-    for (int k = max(k0, C.kg); k < k1; ++k) {
+  for (int k = kw; k < k1; ++k) {
+    const bool act = valid && k >= C.kg;
+    const unsigned m = __ballot_sync(0xffffffffu, act);
+    const bool inter = act && !C.face && k >= C.kint && k < D.nz - 1;
+    const bool all_inter = __ballot_sync(0xffffffffu, inter) == m;
+    if (act) {
       const uint32_t n = (uint32_t)k * D.ps + base;
       Cell<R> X;
-      if (!C.face && k >= C.kint && k < D.nz - 1) stream_interior<S>(D, smem_prof, C, k, n, X);
+      if (all_inter) stream_interior<S>(D, smem_prof, C, k, n, X);
       else stream_cell<S>(D, P, smem_prof, C, k, n, X);
       Macro<R> M;
       if constexpr (FAST) {
