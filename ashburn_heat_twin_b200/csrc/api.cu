@@ -445,6 +445,7 @@ ahx_status ahx_step(ahx_handle* h, int n, int mode) {
   L.block_y = h->block_y;
   L.zslab = h->zslab;
   L.minb = h->minb;
+  L.pairs = h->pairs;
   L.tma_ty = h->maps_ok ? h->tma_ty : 0;
   L.tma_depth = h->tma_depth;
   for (int s = 0; s < n; ++s) {
@@ -766,24 +767,33 @@ ahx_status ahx_set_launch(ahx_handle* h, int block_y, int zslab) {
   if (!h) return fail(AHX_EINVAL, "live solver: null handle");
   std::lock_guard<std::mutex> lk(h->mu);
   if (ahx_status st = check(h)) return st;
+  const bool pairs = block_y >= 2000;   // paired levels: 2000 + the plain encoding
+  if (pairs) {
+    if (h->dims.arith != AHX_ARITH_FAST || h->dims.precision == AHX_FP64)
+      return fail(AHX_EINVAL, "live solver: paired levels need the FMA build and f32 arithmetic");
+    block_y -= 2000;
+  }
   if (block_y >= 1000) {   // staged kernel: 1000 + 100 x depth + rows (4 with depth 2-4, or 8 with depth 2-3)
     const int ty = block_y % 100, dp = (block_y / 100) % 10;
     if (!((ty == 4 && dp >= 2 && dp <= 4) || (ty == 8 && dp >= 2 && dp <= 3)) || zslab < 0)
       return fail(AHX_EINVAL, "live solver: bad staged launch shape");
     if (!h->maps_ok) return fail(AHX_EINVAL, "live solver: tensor maps unavailable for the staged kernel");
+    if (pairs) return fail(AHX_EINVAL, "live solver: the staged kernel has no paired variant");
     h->tma_ty = ty;
     h->tma_depth = dp;
     h->block_y = ty;
     h->minb = 0;
+    h->pairs = false;
   } else {
     const int by = block_y % 100, mb = block_y / 100;
     if (by < 0 || by > 8 || zslab < 0 || (mb != 0 && (mb < 4 || mb > 6)) || (mb && by != 4))
       return fail(AHX_EINVAL, "live solver: bad launch shape");
-    if (block_y) {
-      h->block_y = by;
+    if (block_y || pairs) {
+      h->block_y = by ? by : 4;
       h->minb = mb;
       h->tma_ty = 0;
       h->tma_depth = 0;
+      h->pairs = pairs;
     }
   }
   if (zslab) h->zslab = zslab;
@@ -815,8 +825,12 @@ ahx_status ahx_autotune(ahx_handle* h, int steps_per_trial, int* best_block_y, i
   cudaEventCreate(&e1);
   struct Shape {
     int by, minb, ty, depth;
+    bool pairs;
   };
-  std::vector<Shape> shapes = {{2, 0, 0, 0}, {4, 0, 0, 0}, {8, 0, 0, 0}, {4, 4, 0, 0}, {4, 5, 0, 0}, {4, 6, 0, 0}};
+  std::vector<Shape> shapes = {{2, 0, 0, 0, false}, {4, 0, 0, 0, false}, {8, 0, 0, 0, false},
+                               {4, 4, 0, 0, false}, {4, 5, 0, 0, false}, {4, 6, 0, 0, false}};
+  if (h->dims.arith == AHX_ARITH_FAST && h->dims.precision != AHX_FP64)
+    for (Shape sh : {Shape{4, 4, 0, 0, true}, Shape{4, 5, 0, 0, true}, Shape{4, 6, 0, 0, true}}) shapes.push_back(sh);
   // staged (TMA) shapes, with tensor maps over the scratch copies the trials step
   TmaMaps tm[2][2];
   bool tma_ok = h->maps_ok;
@@ -824,11 +838,13 @@ ahx_status ahx_autotune(ahx_handle* h, int steps_per_trial, int* best_block_y, i
     tma_ok = make_maps(h, f0, g0, t ? 8 : 4, &tm[t][0]) && make_maps(h, f1, g1, t ? 8 : 4, &tm[t][1]);
   }
   if (tma_ok)
-    for (Shape sh : {Shape{4, 0, 4, 2}, Shape{4, 0, 4, 3}, Shape{4, 0, 4, 4}, Shape{8, 0, 8, 2}, Shape{8, 0, 8, 3}})
+    for (Shape sh : {Shape{4, 0, 4, 2, false}, Shape{4, 0, 4, 3, false}, Shape{4, 0, 4, 4, false},
+                     Shape{8, 0, 8, 2, false}, Shape{8, 0, 8, 3, false}})
       shapes.push_back(sh);
   std::vector<int> zss = {h->dims.nz, 32, 16, 8};
   float best = 1e30f;
   int bby = h->block_y, bzs = h->zslab, bmb = h->minb, bty = h->tma_ty, bdp = h->tma_depth;
+  bool bpr = h->pairs;
   DomainView D = view(h);
   D.dbg = nullptr;
   StepLaunch L;
@@ -842,6 +858,7 @@ ahx_status ahx_autotune(ahx_handle* h, int steps_per_trial, int* best_block_y, i
       if (sh.ty && zs < 16) continue;   // the staged kernel needs a few levels per block to fill its pipeline
       L.block_y = sh.by;
       L.minb = sh.minb;
+      L.pairs = sh.pairs;
       L.tma_ty = sh.ty;
       L.tma_depth = sh.depth;
       L.zslab = zs;
@@ -864,8 +881,8 @@ ahx_status ahx_autotune(ahx_handle* h, int steps_per_trial, int* best_block_y, i
           const cudaError_t e2 = cudaStreamSynchronize(h->s_step);
           if (e2 != cudaSuccess) {
             char what[96];
-            std::snprintf(what, sizeof(what), "autotune trial (rows %d, variant %d, staged %d/%d, zslab %d)", sh.by,
-                          sh.minb, sh.ty, sh.depth, zs);
+            std::snprintf(what, sizeof(what), "autotune trial (rows %d, variant %d, staged %d/%d, paired %d, zslab %d)",
+                          sh.by, sh.minb, sh.ty, sh.depth, (int)sh.pairs, zs);
             st = cuda_fail(h, e2, what);
             break;
           }
@@ -883,6 +900,7 @@ ahx_status ahx_autotune(ahx_handle* h, int steps_per_trial, int* best_block_y, i
         bmb = sh.minb;
         bty = sh.ty;
         bdp = sh.depth;
+        bpr = sh.pairs;
       }
     }
   }
@@ -900,8 +918,10 @@ ahx_status ahx_autotune(ahx_handle* h, int steps_per_trial, int* best_block_y, i
   h->minb = bmb;
   h->tma_ty = bty;
   h->tma_depth = bdp;
-  // the ahx_set_launch encoding: variant x 100 + block_y, or 1000 + 100 x depth + rows for the staged kernel
-  if (best_block_y) *best_block_y = bty ? 1000 + 100 * bdp + bty : bmb * 100 + bby;
+  h->pairs = bpr;
+  // the ahx_set_launch encoding: variant x 100 + block_y (+ 2000 for paired levels), or 1000 + 100 x depth + rows for
+  // the staged kernel
+  if (best_block_y) *best_block_y = bty ? 1000 + 100 * bdp + bty : (bpr ? 2000 : 0) + bmb * 100 + bby;
   if (best_zslab) *best_zslab = bzs;
   if (best_ms) *best_ms = best;
   return AHX_OK;

@@ -43,6 +43,7 @@ struct ahx_batch {
   bool destroyed = false, lost = false;
   std::string lost_msg;
   int dev = 0, precision = 0, arith = 0, minb = 4, nsm = 0, occ = 0, grid = 0;
+  bool pairs = false;              // paired levels on packed f32x2 arithmetic (FMA build)
   int cap_members = 0, cap_nz = 0;
   int64_t cap_tiles = 0;
   std::vector<ahx_handle*> members;
@@ -95,6 +96,7 @@ BatchLaunch launch_args(const ahx_batch* b, int set) {
   BatchLaunch L{};
   L.precision = b->precision;
   L.minb = b->minb;
+  L.pairs = b->pairs;
   L.max_nz = b->cap_nz;
   L.grid = b->grid;
   L.views = b->d_views + (size_t)set * b->cap_members;
@@ -406,7 +408,7 @@ ahx_status ahx_batch_set_members(ahx_batch* b, ahx_handle* const* members, int c
   return AHX_OK;
 }
 
-ahx_status ahx_batch_set_launch(ahx_batch* b, int minb, int zslab, int use_graph) {
+ahx_status ahx_batch_set_launch(ahx_batch* b, int minb, int zslab, int use_graph, int pairs) {
   if (!b) return fail(AHX_EINVAL, "live solver: null batch");
   std::lock_guard<std::mutex> lk(b->mu);
   if (ahx_status st = check_batch(b)) return st;
@@ -414,17 +416,23 @@ ahx_status ahx_batch_set_launch(ahx_batch* b, int minb, int zslab, int use_graph
     return fail(AHX_EINVAL, "live solver: batch register-budget variant must be 4, 5 or 6 (0 = keep)");
   if (zslab < -1) return fail(AHX_EINVAL, "live solver: batch z-slab must be > 0, 0 (keep) or -1 (automatic)");
   AHX_BCUDA(b, cudaSetDevice(b->dev));
-  if (minb != 0 && minb != b->minb) {
+  if (pairs > 0 && (b->arith != AHX_ARITH_FAST || b->precision == AHX_FP64))
+    return fail(AHX_EINVAL, "live solver: paired levels need the FMA build and f32 arithmetic");
+  const bool new_pairs = pairs < 0 ? b->pairs : pairs > 0;
+  if ((minb != 0 && minb != b->minb) || new_pairs != b->pairs) {
     AHX_BCUDA(b, cudaStreamSynchronize(b->s));
     const int old = b->minb;
-    b->minb = minb;
+    const bool old_pairs = b->pairs;
+    if (minb != 0) b->minb = minb;
+    b->pairs = new_pairs;
     if (ahx_status st = resize_grid(b)) {
       b->minb = old;
+      b->pairs = old_pairs;
       resize_grid(b);
       return st;
     }
   }
-  if (zslab != 0 || minb != 0) {
+  if (zslab != 0 || minb != 0 || pairs >= 0) {
     if (zslab != 0) b->zs_policy = zslab;
     MemberLocks lock(b->members);
     if (ahx_status st = install(b, b->members)) return st;
@@ -544,6 +552,7 @@ ahx_status ahx_batch_get_info(ahx_batch* b, ahx_batch_info_out* out) {
   out->grid = b->grid;
   out->minb = b->minb;
   out->use_graph = b->use_graph ? 1 : 0;
+  out->pairs = b->pairs ? 1 : 0;
   out->zslab_max = b->zslab.empty() ? 0 : *std::max_element(b->zslab.begin(), b->zslab.end());
   out->cells = b->cells;
   return check_batch(b);

@@ -20,7 +20,10 @@
 //   * reads use the non-coherent path (the source buffer is read-only during a step), writes are streaming stores.
 #pragma once
 
+#include <type_traits>
+
 #include "lattice.cuh"
+#include "lanes.cuh"
 
 namespace ahx {
 
@@ -157,6 +160,22 @@ struct Cell {
   R uI, vI, kb;
 };
 
+// Round-to-nearest operations the compiler cannot contract. The face formulas below use them so the FMA build gives
+// the same bits in every kernel variant (its contraction choices may differ between instantiations); in the exact
+// build they evaluate exactly as the plain operators in the same order.
+__device__ __forceinline__ float nmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float nadd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float nsub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ double nmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double nadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double nsub(double a, double b) { return __dsub_rn(a, b); }
+
+// 1 + 3 cu + 4.5 cu^2 - 1.5 usq, left to right as the reference writes it
+template <class R>
+__device__ __forceinline__ R feq_poly(R cu, R usq) {
+  return nsub(nadd(nadd(R(1.0), nmul(R(3.0), cu)), nmul(nmul(R(4.5), cu), cu)), nmul(R(1.5), usq));
+}
+
 // secProfile + secOutflowPrelude + secStreamF + secStreamG for cell (C.i, C.j, k); n is the pitched cell index.
 template <class S>
 __device__ __forceinline__ void stream_cell(const DomainView& D, const ParamsHead& P, const float4* prof,
@@ -236,7 +255,7 @@ __device__ __forceinline__ void stream_cell(const DomainView& D, const ParamsHea
       uyn = moment1<R, 1>(fo) / rn;
       uzn = moment1<R, 2>(fo) / rn;
     }
-    const R usqn = uxn * uxn + uyn * uyn + uzn * uzn;
+    const R usqn = nadd(nadd(nmul(uxn, uxn), nmul(uyn, uyn)), nmul(uzn, uzn));
     R uxc = uxn, uyc = uyn;
     if (P.oclip != 0) {
       if (C.latW && P.inflow_w == 0 && uxc > R(0)) uxc = R(0);
@@ -244,7 +263,7 @@ __device__ __forceinline__ void stream_cell(const DomainView& D, const ParamsHea
       if (C.latS && P.inflow_s == 0 && uyc > R(0)) uyc = R(0);
       if (C.latN && P.inflow_n == 0 && uyc < R(0)) uyc = R(0);
     }
-    const R usqc = uxc * uxc + uyc * uyc + uzn * uzn;
+    const R usqc = nadd(nadd(nmul(uxc, uxc), nmul(uyc, uyc)), nmul(uzn, uzn));
     static_for<18>([&](auto Qm1) {
       constexpr int q = Qm1 + 1;
       constexpr int cx = kC19[q][0], cy = kC19[q][1], cz = kC19[q][2];
@@ -253,15 +272,14 @@ __device__ __forceinline__ void stream_cell(const DomainView& D, const ParamsHea
           const R w = R(w19(q));
           if (inflow_cond<cx, cy>(C, P)) {
             const R cu = cdot<R, cx, cy, 0>(uI, vI, R(0));
-            X.f[q] = w * (R(1.0) + R(3.0) * cu + R(4.5) * cu * cu - R(1.5) * (uI * uI + vI * vI));
+            X.f[q] = nmul(w, feq_poly(cu, nadd(nmul(uI, uI), nmul(vI, vI))));
           } else {
             const R cu = cdot<R, cx, cy, cz>(uxn, uyn, uzn);
             if (P.oclip != 0) {
               const R cuc = cdot<R, cx, cy, cz>(uxc, uyc, uzn);
-              X.f[q] = X.f[q] + w * ((R(1.0) + R(3.0) * cuc + R(4.5) * cuc * cuc - R(1.5) * usqc) -
-                                     rn * (R(1.0) + R(3.0) * cu + R(4.5) * cu * cu - R(1.5) * usqn));
+              X.f[q] = nadd(X.f[q], nmul(w, nsub(feq_poly(cuc, usqc), nmul(rn, feq_poly(cu, usqn)))));
             } else {
-              X.f[q] = X.f[q] + w * (R(1.0) - rn) * (R(1.0) + R(3.0) * cu + R(4.5) * cu * cu - R(1.5) * usqn);
+              X.f[q] = nadd(X.f[q], nmul(nmul(w, nsub(R(1.0), rn)), feq_poly(cu, usqn)));
             }
           }
         }
@@ -372,7 +390,6 @@ __device__ __forceinline__ void collide_store(const DomainView& D, const ParamsH
   using KG = CodecG<S>;
   StoreF<S>* fB = static_cast<StoreF<S>*>(D.fB);
   StoreG<S>* gB = static_cast<StoreG<S>*>(D.gB);
-  const uint32_t qs = D.qs;
   const R rho = M.rho, ux = M.ux, uy = M.uy, uz = M.uz, Fx = M.Fx, Fy = M.Fy, Fz = M.Fz;
   const R* f = X.f;
   const R Pxx = moment2<R, 0, 0>(f), Pyy = moment2<R, 1, 1>(f), Pzz = moment2<R, 2, 2>(f);
@@ -433,10 +450,23 @@ __device__ __forceinline__ void collide_store(const DomainView& D, const ParamsH
   });
 }
 
-// The same relaxation in the contracted build, rearranged: each population q is paired with its opposite (adjacent
-// in the velocity table), the even and odd parts of the equilibrium, the regularised non-equilibrium term (even in c)
-// and the Guo forcing are formed once per pair, and 1/rho, 1/tau are taken once. Mathematically identical to
-// moments_forces + collide_store; rounding differs (held to the single-step theta rel-L2 <= 1e-5 bar).
+// Top-sponge strength at level k (secForces, kernel.js:296-304): sigmax a^2 with a = (k - (nz - nsp) + 1) / nsp in
+// the top nsp levels, else 0. One definition for the single-cell and the paired FMA paths.
+__device__ __forceinline__ float sponge_sg(const ParamsHead& P, int nz, int k) {
+  if (k < nz - P.nsp) return 0.0f;
+  const float aa = __fdividef(__fadd_rn((float)(k - (nz - P.nsp)), 1.0f), (float)P.nsp);
+  return __fmul_rn(__fmul_rn(P.sigmax, aa), aa);
+}
+__device__ __forceinline__ double sponge_sg_d(const ParamsHead& P, int nz, int k) {
+  if (k < nz - P.nsp) return 0.0;
+  const double aa = ((double)(k - (nz - P.nsp)) + 1.0) / (double)P.nsp;
+  return (double)P.sigmax * aa * aa;
+}
+
+// The relaxation of the FMA build (lanes.cuh) for one cell: each population q is paired with its opposite, the even
+// and odd parts of the equilibrium, the regularised non-equilibrium term and the Guo forcing are formed once per
+// pair, and 1/rho, 1/tau are taken once. Mathematically identical to moments_forces + collide_store; rounding
+// differs (held to the single-step theta rel-L2 <= 1e-5 bar).
 template <class S>
 __device__ __forceinline__ void fast_update(const DomainView& D, const ParamsHead& P,
                                             const Column<RealOf<S>>& C, int k, uint32_t n,
@@ -447,121 +477,127 @@ __device__ __forceinline__ void fast_update(const DomainView& D, const ParamsHea
   using KG = CodecG<S>;
   StoreF<S>* fB = static_cast<StoreF<S>*>(D.fB);
   StoreG<S>* gB = static_cast<StoreG<S>*>(D.gB);
-  const uint32_t qs = D.qs;
-  R sp9[9], dp9[9];
-  static_for<9>([&](auto Pi) {
-    constexpr int p = Pi;
-    sp9[p] = X.f[2 * p + 1] + X.f[2 * p + 2];
-    dp9[p] = X.f[2 * p + 1] - X.f[2 * p + 2];
-  });
-  R rho = X.f[0];
-#pragma unroll
-  for (int p = 0; p < 9; ++p) rho += sp9[p];
-  R jx = R(0), jy = R(0), jz = R(0), Pxx = R(0), Pyy = R(0), Pzz = R(0), Pxy = R(0), Pxz = R(0), Pyz = R(0);
-  static_for<9>([&](auto Pi) {
-    constexpr int p = Pi;
-    constexpr int q = 2 * p + 1;
-    constexpr int cx = kC19[q][0], cy = kC19[q][1], cz = kC19[q][2];
-    if constexpr (cx != 0) { jx += R(cx) * dp9[p]; Pxx += sp9[p]; }
-    if constexpr (cy != 0) { jy += R(cy) * dp9[p]; Pyy += sp9[p]; }
-    if constexpr (cz != 0) { jz += R(cz) * dp9[p]; Pzz += sp9[p]; }
-    if constexpr (cx != 0 && cy != 0) Pxy += R(cx * cy) * sp9[p];
-    if constexpr (cx != 0 && cz != 0) Pxz += R(cx * cz) * sp9[p];
-    if constexpr (cy != 0 && cz != 0) Pyz += R(cy * cz) * sp9[p];
-  });
-  const R th = X.g[0] + (X.g[1] + X.g[2]) + (X.g[3] + X.g[4]) + (X.g[5] + X.g[6]);
-  const R irho = R(1) / rho;
-  R Fx = R(0), Fy = R(0), Fz = rho * R(P.gbeta) * th;
+  Moments<R> m;
+  lane_moments<R>(X.f, X.g, m);
+  R Fx0 = R(0), Fy0 = R(0);
   if (k == C.kg && C.kg == C.ktc) {
-    const R ux0 = jx * irho, uy0 = jy * irho;
-    const R sp = sqrt(ux0 * ux0 + uy0 * uy0);
-    const R cd = R(C.cd);
-    const R a = (cd * sp > R(0.5)) ? R(-0.5) * rho : -rho * cd * sp;   // implicit-limited log-law drag
-    Fx = a * ux0;
-    Fy = a * uy0;
+    // implicit-limited log-law drag on the first fluid cell of a building-free column
+    const R ux0 = vmul(m.jx, m.irho), uy0 = vmul(m.jy, m.irho);
+    const R csp = vmul(R(C.cd), vsqrt(vfma(uy0, uy0, vmul(ux0, ux0))));
+    const R a = csp > R(0.5) ? vmul(R(-0.5), m.rho) : vsub(R(0), vmul(m.rho, csp));
+    Fx0 = vmul(a, ux0);
+    Fy0 = vmul(a, uy0);
   }
-  R sg = R(0);
-  if (k >= D.nz - P.nsp) {
-    const R aa = (R(k - (D.nz - P.nsp)) + R(1.0)) / R(P.nsp);
-    sg = R(P.sigmax) * aa * aa;
-    const R rs = rho * sg;
-    Fx += rs * (X.uI - jx * irho);
-    Fy += rs * (X.vI - jy * irho);
-    Fz -= rs * (jz * irho);
-  }
-  const R ux = (jx + R(0.5) * Fx) * irho, uy = (jy + R(0.5) * Fy) * irho, uz = (jz + R(0.5) * Fz) * irho;
-  const R usq = ux * ux + uy * uy + uz * uz;
-  const R r3 = rho * R(1.0 / 3.0);
-  const R Nxx = Pxx - r3 - rho * ux * ux;
-  const R Nyy = Pyy - r3 - rho * uy * uy;
-  const R Nzz = Pzz - r3 - rho * uz * uz;
-  const R Nxy = Pxy - rho * ux * uy;
-  const R Nxz = Pxz - rho * ux * uz;
-  const R Nyz = Pyz - rho * uy * uz;
-  const R Pn = sqrt(Nxx * Nxx + Nyy * Nyy + Nzz * Nzz + R(2.0) * (Nxy * Nxy + Nxz * Nxz + Nyz * Nyz));
-  R tb = R(P.tau0) + R(3.0) * R(P.momfac) * X.kb;
-  if (C.spon) tb += C.spg;
-  const R tau = R(0.5) * (tb + sqrt(tb * tb + R(P.cs2smag) * Pn * irho));
-  const R itau = R(1) / tau;
-  const R nusgs = (tau - tb) * R(1.0 / 3.0);
-  const R kap = nusgs / R(P.prt) + X.kb + R(P.kfloor);
-  const R taug = R(0.5) + R(4.0) * kap;
-  const R om = R(1.0) - itau;
-  const R fpre = R(1.0) - R(0.5) * itau;
-  const R trN = (Nxx + Nyy + Nzz) * R(1.0 / 3.0);
-  const R uF = ux * Fx + uy * Fy + uz * Fz;
-  const R base = R(1.0) - R(1.5) * usq;
-  // q = 0
-  {
-    const R w = R(w19(0));
-    const R f0 = w * rho * base + om * R(4.5 * w19(0)) * (-trN) + fpre * w * (R(-3.0) * uF);
-    KF::store(fB + n, KF::enc_f(f0, w));
-  }
-  static_for<9>([&](auto Pi) {
-    constexpr int p = Pi;
-    constexpr int q = 2 * p + 1;
-    constexpr int cx = kC19[q][0], cy = kC19[q][1], cz = kC19[q][2];
-    const R w = R(w19(q));
-    const R cu = cdot<R, cx, cy, cz>(ux, uy, uz);
-    const R cF = cdot<R, cx, cy, cz>(Fx, Fy, Fz);
-    R qn = R(0);
-    if constexpr (cx != 0) qn += Nxx;
-    if constexpr (cy != 0) qn += Nyy;
-    if constexpr (cz != 0) qn += Nzz;
-    if constexpr (cx != 0 && cy != 0) qn += R(2 * cx * cy) * Nxy;
-    if constexpr (cx != 0 && cz != 0) qn += R(2 * cx * cz) * Nxz;
-    if constexpr (cy != 0 && cz != 0) qn += R(2 * cy * cz) * Nyz;
-    const R rw = rho * w, fw = fpre * w;
-    const R E = rw * (base + R(4.5) * cu * cu) + om * R(4.5 * w19(q)) * (qn - trN) + fw * (R(9.0) * cu * cF - R(3.0) * uF);
-    const R O = R(3.0) * (rw * cu + fw * cF);
-    KF::store(fB + (n + D.plane[q]), KF::enc_f(E + O, w));
-    KF::store(fB + (n + D.plane[q + 1]), KF::enc_f(E - O, w));
-  });
-  const R Ssrc = (k == C.kg) ? R(C.qsrc) * R(P.srcscale) : R(0);
-  const R omg = R(1.0) / taug;
-  const R a = R(1.0) - omg, one_sg = R(1.0) - sg;
-  KG::store(gB + n, KG::enc_g((a * X.g[0] + omg * R(w7(0)) * th + R(w7(0)) * Ssrc) * one_sg));
-  static_for<3>([&](auto Pi) {
-    constexpr int p = Pi;
-    constexpr int q = 2 * p + 1;
-    constexpr int cx = kC7[q][0], cy = kC7[q][1], cz = kC7[q][2];
-    const R b = omg * R(w7(q)) * th + R(w7(q)) * Ssrc;
-    const R c4 = omg * R(4.0 * w7(q)) * th * cdot<R, cx, cy, cz>(ux, uy, uz);
-    KG::store(gB + (n + D.plane[q]), KG::enc_g((a * X.g[q] + b + c4) * one_sg));
-    KG::store(gB + (n + D.plane[q + 1]), KG::enc_g((a * X.g[q + 1] + b - c4) * one_sg));
-  });
-  M.rho = rho;
-  M.jx = jx;
-  M.jy = jy;
-  M.jz = jz;
-  M.th = th;
-  M.Fx = Fx;
-  M.Fy = Fy;
-  M.Fz = Fz;
+  R sg;
+  if constexpr (sizeof(R) == 8) sg = sponge_sg_d(P, D.nz, k);
+  else sg = sponge_sg(P, D.nz, k);
+  const R Ssrc = (k == C.kg) ? vmul(R(C.qsrc), R(P.srcscale)) : R(0);
+  const R tb_add = C.spon ? R(C.spg) : R(0);
+  Relaxed<R> o;
+  lane_relax<R>(
+      P, m, X.g, X.uI, X.vI, X.kb, sg, Fx0, Fy0, Ssrc, tb_add, o,
+      [&](auto Q, R v) {
+        constexpr int q = Q;
+        KF::store(fB + (q == 0 ? n : n + D.plane[q]), KF::enc_f(v, R(w19(q))));
+      },
+      [&](auto Q, R v) {
+        constexpr int q = Q;
+        KG::store(gB + (q == 0 ? n : n + D.plane[q]), KG::enc_g(v));
+      });
+  M.rho = m.rho;
+  M.jx = m.jx;
+  M.jy = m.jy;
+  M.jz = m.jz;
+  M.th = m.th;
+  M.Fx = o.Fx;
+  M.Fy = o.Fy;
+  M.Fz = o.Fz;
   M.sg = sg;
-  M.ux = ux;
-  M.uy = uy;
-  M.uz = uz;
+  M.ux = o.ux;
+  M.uy = o.uy;
+  M.uz = o.uz;
+}
+
+// paired load / store of one population of cells n and n + ps, decoded / encoded exactly as the single-cell codec
+template <class T>
+__device__ __forceinline__ float2 pair_load_f(const T* p, uint32_t ps, float w) {
+  using K = Codec<T>;
+  if constexpr (K::kBytes == 2)
+    return vfma(make_float2(K::raw(K::load(p)), K::raw(K::load(p + ps))), vc<float2>(1.0 / K::kF), vc<float2>(w));
+  else
+    return make_float2(K::load(p), K::load(p + ps));
+}
+template <class T>
+__device__ __forceinline__ float2 pair_load_g(const T* p, uint32_t ps) {
+  using K = Codec<T>;
+  if constexpr (K::kBytes == 2)
+    return vmul(make_float2(K::raw(K::load(p)), K::raw(K::load(p + ps))), vc<float2>(1.0 / K::kG));
+  else
+    return make_float2(K::load(p), K::load(p + ps));
+}
+template <class T>
+__device__ __forceinline__ void pair_store_f(T* p, uint32_t ps, float2 v, float w) {
+  using K = Codec<T>;
+  if constexpr (K::kBytes == 2) {
+    const float2 e = vfma(v, vc<float2>(K::kF), vc<float2>(-(double)K::kF * w));
+    K::store(p, K::cvt(e.x));
+    K::store(p + ps, K::cvt(e.y));
+  } else {
+    K::store(p, v.x);
+    K::store(p + ps, v.y);
+  }
+}
+template <class T>
+__device__ __forceinline__ void pair_store_g(T* p, uint32_t ps, float2 v) {
+  using K = Codec<T>;
+  if constexpr (K::kBytes == 2) {
+    const float2 e = vmul(v, vc<float2>(K::kG));
+    K::store(p, K::cvt(e.x));
+    K::store(p + ps, K::cvt(e.y));
+  } else {
+    K::store(p, v.x);
+    K::store(p + ps, v.y);
+  }
+}
+
+// Two vertically adjacent interior cells (k, k + 1) of one column, streamed and relaxed as the two lanes of packed
+// f32x2 arithmetic. Interior cells are never the first fluid cell (no drag, no source); the result of each lane is
+// bit-identical to stream_interior + fast_update on that cell alone.
+template <class S>
+__device__ __forceinline__ void fast_pair(const DomainView& D, const ParamsHead& P, const float4* prof,
+                                          const Column<float>& C, int k, uint32_t n) {
+  const StoreF<S>* fA = static_cast<const StoreF<S>*>(D.fA);
+  const StoreG<S>* gA = static_cast<const StoreG<S>*>(D.gA);
+  StoreF<S>* fB = static_cast<StoreF<S>*>(D.fB);
+  StoreG<S>* gB = static_cast<StoreG<S>*>(D.gB);
+  const uint32_t ps = D.ps;
+  float2 f[19], g[7];
+  static_for<19>([&](auto Q) {
+    constexpr int q = Q;
+    f[q] = pair_load_f(fA + (n + D.pull_f[q]), ps, (float)w19(q));
+  });
+  static_for<7>([&](auto Q) {
+    constexpr int q = Q;
+    g[q] = pair_load_g(gA + (n + D.pull_g[q]), ps);
+  });
+  const int z0 = min(max(k - C.ktc, 0), D.nz - 1), z1 = min(max(k + 1 - C.ktc, 0), D.nz - 1);
+  const float4 p0 = prof[z0], p1 = prof[z1];
+  Moments<float2> m;
+  lane_moments<float2>(f, g, m);
+  const float2 zero = vc<float2>(0.0);
+  const float2 tb_add = C.spon ? vc<float2>(C.spg) : zero;
+  Relaxed<float2> o;
+  lane_relax<float2>(
+      P, m, g, make_float2(p0.x, p1.x), make_float2(p0.y, p1.y), make_float2(p0.z, p1.z),
+      make_float2(sponge_sg(P, D.nz, k), sponge_sg(P, D.nz, k + 1)), zero, zero, zero, tb_add, o,
+      [&](auto Q, float2 v) {
+        constexpr int q = Q;
+        pair_store_f(fB + (q == 0 ? n : n + D.plane[q]), ps, v, (float)w19(q));
+      },
+      [&](auto Q, float2 v) {
+        constexpr int q = Q;
+        pair_store_g(gB + (q == 0 ? n : n + D.plane[q]), ps, v);
+      });
 }
 
 // Budget accumulators of one thread (summed over its cells, then reduced per block into FP64).
@@ -573,7 +609,7 @@ struct BudgetAcc {
 constexpr int kBlockX = 32;
 
 // The fused step over one z-slab of the columns of a block. MODE: 0 none, 1 write dbg, 2 accumulate dbg.
-template <class S, int MODE, bool BUDGET, bool FAST>
+template <class S, int MODE, bool BUDGET, bool FAST, bool PAIRS = false>
 __device__ __forceinline__ void step_block(const DomainView& D, int bx, int by, int bz, int zslab) {
   using R = RealOf<S>;
   extern __shared__ float4 smem_prof[];
@@ -608,8 +644,22 @@ __device__ __forceinline__ void step_block(const DomainView& D, int bx, int by, 
   }
   const int kw = __reduce_min_sync(0xffffffffu, kstart);
   const uint32_t base = (uint32_t)j * (uint32_t)D.px + (uint32_t)i;
+  // PAIRS (FMA build without output modes): two interior levels at a time on the packed f32x2 lanes when every
+  // active lane of the warp has both cells interior (bit-identical to the single-level path; more registers)
+  constexpr bool kPairs = PAIRS && FAST && MODE == 0 && !BUDGET && std::is_same_v<R, float>;
 #pragma unroll 1
   for (int k = kw; k < k1; ++k) {
+    if constexpr (kPairs) {
+      if (k + 1 < k1) {
+        const bool in2 = valid && k >= C.kg && !C.face && k >= C.kint && k + 1 < D.nz - 1;
+        const unsigned m2 = __ballot_sync(0xffffffffu, valid && k + 1 >= C.kg);
+        if (m2 != 0u && __ballot_sync(0xffffffffu, in2) == m2) {
+          if (in2) fast_pair<S>(D, P, smem_prof, C, k, (uint32_t)k * D.ps + base);
+          ++k;
+          continue;
+        }
+      }
+    }
     const bool act = valid && k >= C.kg;
     const unsigned m = __ballot_sync(0xffffffffu, act);
     const bool inter = act && !C.face && k >= C.kint && k < D.nz - 1;

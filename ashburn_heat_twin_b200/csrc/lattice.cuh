@@ -103,6 +103,10 @@ struct Codec<__half> {
     return __float2half_rn(__fmaf_rn(v, kScaleF16, -kScaleF16 * w));
   }
   __device__ __forceinline__ static __half enc_g(float v) { return __float2half_rn(__fmul_rn(v, kScaleG16)); }
+  // the pieces of the codec, for paired (two-lane) decoding and encoding with identical rounding
+  static constexpr float kF = kScaleF16, kG = kScaleG16;
+  __device__ __forceinline__ static float raw(__half v) { return __half2float(v); }
+  __device__ __forceinline__ static __half cvt(float v) { return __float2half_rn(v); }
 };
 
 template <>
@@ -127,6 +131,10 @@ struct Codec<__nv_bfloat16> {
   __device__ __forceinline__ static __nv_bfloat16 enc_g(float v) {
     return __float2bfloat16_rn(__fmul_rn(v, kScaleBF16));
   }
+  // the pieces of the codec, for paired (two-lane) decoding and encoding with identical rounding
+  static constexpr float kF = kScaleBF16, kG = kScaleBF16;
+  __device__ __forceinline__ static float raw(__nv_bfloat16 v) { return __bfloat162float(v); }
+  __device__ __forceinline__ static __nv_bfloat16 cvt(float v) { return __float2bfloat16_rn(v); }
 };
 
 // Storage of a state: a plain type stores f and g alike; Mixed<SF, SG> stores the flow populations f as SF and the

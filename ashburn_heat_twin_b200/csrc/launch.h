@@ -18,6 +18,7 @@ struct StepLaunch {
   int block_y;     // threads per block in y (x is one warp)
   int zslab;       // levels per block
   int minb = 0;    // 0, or 4 / 5 / 6 resident 128-thread blocks per SM (register budget 128 / 96 / 80)
+  bool pairs = false;   // FMA build: two interior levels per thread on packed f32x2 arithmetic
   int tma_ty = 0;  // > 0: the TMA-staged kernel with 32 x tma_ty columns per block ...
   int tma_depth = 0;               // ... and this many levels staged ahead
   const TmaMaps* maps = nullptr;   // tensor maps of the state being read
@@ -31,6 +32,7 @@ struct BatchTile {
 struct BatchLaunch {
   int precision;                 // ahx_precision, the same for every member
   int minb;                      // 4 / 5 / 6 resident 128-thread blocks per SM
+  bool pairs;                    // FMA build: two interior levels per thread on packed f32x2 arithmetic
   int max_nz;                    // level capacity (sizes the staged inflow profile in shared memory)
   int grid;                      // persistent blocks
   const DomainView* views;       // device: one view per member

@@ -18,9 +18,9 @@ namespace AHX_STEP_NS {
 
 // MINB = 0: up to 256 threads per block, registers as the compiler likes; MINB = 4 / 5 / 6: 128-thread blocks with
 // 4 / 5 / 6 resident per SM (a 128 / 96 / 80 register budget), chosen by the launch-shape tuner
-template <class S, int MODE, bool BUDGET, int MINB>
+template <class S, int MODE, bool BUDGET, int MINB, bool PAIRS = false>
 __global__ void __launch_bounds__(MINB ? 128 : 256, MINB ? MINB : 1) step_kernel(DomainView D, int zslab) {
-  step_block<S, MODE, BUDGET, AHX_STEP_FAST != 0>(D, blockIdx.x, blockIdx.y, blockIdx.z, zslab);
+  step_block<S, MODE, BUDGET, AHX_STEP_FAST != 0, PAIRS>(D, blockIdx.x, blockIdx.y, blockIdx.z, zslab);
 }
 
 template <class S, int TY, int DEPTH>
@@ -35,7 +35,7 @@ __global__ void __launch_bounds__(32 * TY, TY == 4 ? 4 : 2)
 // result is bit-identical to stepping it alone. The tile count is read from device memory, so one captured launch
 // serves any membership the tables describe. The last block to finish resets the counters for the next launch on
 // the stream (launches on one stream do not overlap).
-template <class S, int MINB>
+template <class S, int MINB, bool PAIRS>
 __global__ void __launch_bounds__(128, MINB) batch_kernel(const DomainView* __restrict__ views,
                                                           const BatchTile* __restrict__ tiles,
                                                           const int* __restrict__ zslabs,
@@ -56,7 +56,7 @@ __global__ void __launch_bounds__(128, MINB) batch_kernel(const DomainView* __re
     for (int w = tid; w < (int)(sizeof(DomainView) / 4); w += 128) dst[w] = src[w];
     if (tid == 0) s_zslab = zslabs[T.member];
     __syncthreads();
-    step_block<S, 0, false, AHX_STEP_FAST != 0>(sD, T.bx, T.by, T.bz, s_zslab);
+    step_block<S, 0, false, AHX_STEP_FAST != 0, PAIRS>(sD, T.bx, T.by, T.bz, s_zslab);
     __syncthreads();   // the next tile overwrites the view, the staged profile and s_t
   }
   if (tid == 0) {
@@ -68,21 +68,30 @@ __global__ void __launch_bounds__(128, MINB) batch_kernel(const DomainView* __re
   }
 }
 
-template <class S, int MINB>
+template <class S, int MINB, bool PAIRS>
 static cudaError_t batch_t(const BatchLaunch& B, cudaStream_t s, int* occupancy) {
   const size_t smem = (size_t)B.max_nz * sizeof(float4);
-  if (occupancy) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occupancy, batch_kernel<S, MINB>, 128, smem);
-  batch_kernel<S, MINB><<<B.grid, dim3(32, 4), smem, s>>>(B.views, B.tiles, B.zslabs, B.ntiles, B.sched);
+  if (occupancy)
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occupancy, batch_kernel<S, MINB, PAIRS>, 128, smem);
+  batch_kernel<S, MINB, PAIRS><<<B.grid, dim3(32, 4), smem, s>>>(B.views, B.tiles, B.zslabs, B.ntiles, B.sched);
   return cudaGetLastError();
+}
+
+template <class S, bool PAIRS>
+static cudaError_t batch_m(const BatchLaunch& B, cudaStream_t s, int* occupancy) {
+  switch (B.minb) {
+    case 5: return batch_t<S, 5, PAIRS>(B, s, occupancy);
+    case 6: return batch_t<S, 6, PAIRS>(B, s, occupancy);
+    default: return batch_t<S, 4, PAIRS>(B, s, occupancy);
+  }
 }
 
 template <class S>
 static cudaError_t batch_s(const BatchLaunch& B, cudaStream_t s, int* occupancy) {
-  switch (B.minb) {
-    case 4: return batch_t<S, 4>(B, s, occupancy);
-    case 6: return batch_t<S, 6>(B, s, occupancy);
-    default: return batch_t<S, 5>(B, s, occupancy);
+  if constexpr (AHX_STEP_FAST != 0 && std::is_same_v<RealOf<S>, float>) {
+    if (B.pairs) return batch_m<S, true>(B, s, occupancy);
   }
+  return batch_m<S, false>(B, s, occupancy);
 }
 
 cudaError_t launch_batch(const BatchLaunch& B, cudaStream_t s, int* occupancy) {
@@ -142,6 +151,16 @@ static cudaError_t launch_t(const DomainView& D, const StepLaunch& L, cudaStream
   dim3 block(kBlockX, by);
   dim3 grid((D.nx + kBlockX - 1) / kBlockX, (D.ny + by - 1) / by, (D.nz + zs - 1) / zs);
   const size_t smem = (size_t)D.nz * sizeof(float4);
+  if constexpr (MODE == 0 && !BUDGET && AHX_STEP_FAST != 0 && std::is_same_v<RealOf<S>, float>) {
+    if (L.pairs) {
+      switch (minb) {
+        case 4: step_kernel<S, 0, false, 4, true><<<grid, block, smem, s>>>(D, zs); return cudaGetLastError();
+        case 5: step_kernel<S, 0, false, 5, true><<<grid, block, smem, s>>>(D, zs); return cudaGetLastError();
+        case 6: step_kernel<S, 0, false, 6, true><<<grid, block, smem, s>>>(D, zs); return cudaGetLastError();
+        default: step_kernel<S, 0, false, 0, true><<<grid, block, smem, s>>>(D, zs); return cudaGetLastError();
+      }
+    }
+  }
   if constexpr (MODE == 0 && !BUDGET) {
     if (minb == 4) {
       step_kernel<S, MODE, BUDGET, 4><<<grid, block, smem, s>>>(D, zs);

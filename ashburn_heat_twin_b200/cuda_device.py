@@ -62,7 +62,7 @@ class BudgetOut(ctypes.Structure):
 class BatchInfoOut(ctypes.Structure):
     _fields_ = [('members', ctypes.c_int32), ('tiles', ctypes.c_int32), ('grid', ctypes.c_int32),
                 ('minb', ctypes.c_int32), ('use_graph', ctypes.c_int32), ('zslab_max', ctypes.c_int32),
-                ('cells', ctypes.c_int64)]
+                ('pairs', ctypes.c_int32), ('pad', ctypes.c_int32), ('cells', ctypes.c_int64)]
 
 
 _lib = None
@@ -112,7 +112,7 @@ def load_library(path: str = LIB_PATH):
         'ahx_batch_step': [H, i],
         'ahx_batch_time_steps': [H, i, i, ctypes.POINTER(ctypes.c_float)],
         'ahx_batch_sync': [H, i],
-        'ahx_batch_set_launch': [H, i, i, i],
+        'ahx_batch_set_launch': [H, i, i, i, i],
         'ahx_batch_set_members': [H, ctypes.POINTER(H), i],
         'ahx_batch_get_info': [H, ctypes.POINTER(BatchInfoOut)],
         'ahx_batch_destroy': [H],
@@ -170,6 +170,7 @@ class CudaDevice:
         self.nx, self.ny, self.nz = nx, ny, nz
         self.N = nx * ny * nz
         self.precision = precision
+        self.arith = arith
         info = self.hd.info()
         self.adapter = info['device_name']
         self._p = 0
@@ -385,8 +386,9 @@ class Batch:
     def sync(self, timeout_s=None):
         self._call('ahx_batch_sync', self.b, -1 if timeout_s is None else int(timeout_s * 1000))
 
-    def set_launch(self, minb=0, zslab=0, use_graph=True):
-        self._call('ahx_batch_set_launch', self.b, int(minb), int(zslab), 1 if use_graph else 0)
+    def set_launch(self, minb=0, zslab=0, use_graph=True, pairs=None):
+        self._call('ahx_batch_set_launch', self.b, int(minb), int(zslab), 1 if use_graph else 0,
+                   -1 if pairs is None else int(bool(pairs)))
 
     def set_members(self, devices):
         self.devices = list(devices)
@@ -396,7 +398,7 @@ class Batch:
     def info(self):
         o = BatchInfoOut()
         self._call('ahx_batch_get_info', self.b, ctypes.byref(o))
-        return {k: getattr(o, k) for k, _ in BatchInfoOut._fields_}
+        return {k: getattr(o, k) for k, _ in BatchInfoOut._fields_ if k != 'pad'}
 
     def destroy(self):
         if self.b is not None:

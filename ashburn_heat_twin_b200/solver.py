@@ -552,25 +552,28 @@ class LiveBatch:
         self._advance(n)
         return self._b.info()['cells'] * n / (ms * 1e-3) / 1e6
 
-    def set_launch(self, minb=0, zslab=0, use_graph=True):
-        """register-budget variant (4 / 5 / 6, 0 = keep), tile depth (levels, 0 = keep, -1 = automatic) and graph
-        replay on or off."""
-        self._b.set_launch(minb, zslab, use_graph)
+    def set_launch(self, minb=0, zslab=0, use_graph=True, pairs=None):
+        """register-budget variant (4 / 5 / 6, 0 = keep), tile depth (levels, 0 = keep, -1 = whole columns), graph
+        replay on or off, paired levels on packed f32x2 arithmetic (None = keep)."""
+        self._b.set_launch(minb, zslab, use_graph, pairs)
 
     def autotune(self, steps_per_trial=4):
         """time the register-budget variants x tile depths on the batch itself and keep the fastest. Like
-        benchmark(), the trials advance every member's state (by 6 x (2 + steps_per_trial) steps)."""
+        benchmark(), the trials advance every member's state (by up to 12 x (2 + steps_per_trial) steps)."""
+        paired = (False, True) if self.solvers[0]._dev.arith == 'fast' and self.solvers[0]._dev.precision != 'fp64' \
+            else (False,)
         best = None
-        for minb in (4, 5):
-            for zs in (4, 8, 16):
-                self._b.set_launch(minb, zs, True)
-                self._b.time_steps(2)
-                ms = self._b.time_steps(steps_per_trial)
-                self._advance(2 + steps_per_trial)
-                if best is None or ms < best[0]:
-                    best = (ms, minb, zs)
-        self._b.set_launch(best[1], best[2], True)
-        return dict(minb=best[1], zslab=best[2], ms_per_step=best[0] / steps_per_trial)
+        for pr in paired:
+            for minb in (4, 5):
+                for zs in (4, 8, 16):
+                    self._b.set_launch(minb, zs, True, pr)
+                    self._b.time_steps(2)
+                    ms = self._b.time_steps(steps_per_trial)
+                    self._advance(2 + steps_per_trial)
+                    if best is None or ms < best[0]:
+                        best = (ms, minb, zs, pr)
+        self._b.set_launch(best[1], best[2], True, best[3])
+        return dict(minb=best[1], zslab=best[2], pairs=best[3], ms_per_step=best[0] / steps_per_trial)
 
     def destroy(self):
         """release the batch (idempotent); the members stay alive."""

@@ -189,9 +189,10 @@ ahx_status ahx_budget_read(ahx_handle* h, ahx_budget_out* out, int reset);
 /* --- tuning ----------------------------------------------------------------------------------------------------- */
 
 /* launch shape of the fused step: block_y = threads per block in y (x is one warp) plus 100 x the register-budget
- * variant (0: compiler's choice; 4, 5 or 6: 128-thread blocks, that many resident per SM, only with block_y 4); or,
- * for the TMA-staged kernel, 1000 + 100 x stages + rows (rows 4 with 2-4 stages, rows 8 with 2-3 stages);
- * zslab = z-slab depth in levels; 0 = keep */
+ * variant (0: compiler's choice; 4, 5 or 6: 128-thread blocks, that many resident per SM, only with block_y 4), plus
+ * 2000 for paired levels (two interior levels per thread on packed f32x2 arithmetic; FMA build, f32 arithmetic; the
+ * results are bit-identical to unpaired); or, for the TMA-staged kernel, 1000 + 100 x stages + rows (rows 4 with
+ * 2-4 stages, rows 8 with 2-3 stages); zslab = z-slab depth in levels; 0 = keep */
 ahx_status ahx_set_launch(ahx_handle* h, int block_y, int zslab);
 /* time candidate launch shapes on scratch copies of the state and keep the fastest; the state is not advanced;
  * *best_block_y uses the encoding of ahx_set_launch */
@@ -227,7 +228,7 @@ ahx_status ahx_stats_noalloc(int nx, int ny, int nz, const float* f, const float
 typedef struct ahx_batch ahx_batch;
 
 typedef struct {
-  int members, tiles, grid, minb, use_graph, zslab_max;
+  int members, tiles, grid, minb, use_graph, zslab_max, pairs, pad;
   int64_t cells;   /* sum of nx*ny*nz over the members */
 } ahx_batch_info_out;
 
@@ -244,8 +245,9 @@ ahx_status ahx_batch_time_steps(ahx_batch* b, int n, int timeout_ms, float* ms);
 ahx_status ahx_batch_sync(ahx_batch* b, int timeout_ms);
 /* launch set-up: register-budget variant 4 / 5 / 6 (0 = keep); tile depth zslab in levels for every member (clipped
  * to its nz; 0 = keep; -1 = whole columns when that leaves at least 4 tiles per persistent block, else each member's
- * own z-slab); whether steps replay the captured graph (1) or launch one kernel per step (0) */
-ahx_status ahx_batch_set_launch(ahx_batch* b, int minb, int zslab, int use_graph);
+ * own z-slab); whether steps replay the captured graph (1) or launch one kernel per step (0); paired levels on packed
+ * f32x2 arithmetic (1 on, 0 off, -1 keep; FMA build, f32 arithmetic only) */
+ahx_status ahx_batch_set_launch(ahx_batch* b, int minb, int zslab, int use_graph, int pairs);
 ahx_status ahx_batch_get_info(ahx_batch* b, ahx_batch_info_out* out);
 ahx_status ahx_batch_destroy(ahx_batch* b);   /* idempotent; members are released */
 

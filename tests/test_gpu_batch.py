@@ -90,6 +90,8 @@ def test_batch_variants_agree():
     b2 = LiveBatch(ref)
     b2.set_launch(minb=6, zslab=-1)
     b2.step(4).result()
+    with pytest.raises(Exception, match='paired levels need the FMA build'):
+        b2.set_launch(pairs=True)                  # exact build: no paired variant
     b2.destroy()
     for a, m in zip(ref, mem):
         same(a, m)
@@ -134,4 +136,20 @@ def test_batch_membership_changes_match_solo():
     same(solo[1], mem[1])
     b.destroy()
     for s in solo + mem[1:]:
+        s.destroy()
+
+
+def test_batch_paired_levels_match_solo():
+    solo = [scenario(i, 'fp16', 'fast') for i in range(3)]
+    mem = [scenario(i, 'fp16', 'fast') for i in range(3)]
+    b = LiveBatch(mem)
+    b.set_launch(minb=4, zslab=8, pairs=True)
+    assert b.info['pairs'] == 1
+    b.step(7).result()
+    for s in solo:
+        s.step(7).result()
+    for a, m in zip(solo, mem):
+        same(a, m)
+    b.destroy()
+    for s in solo + mem:
         s.destroy()
