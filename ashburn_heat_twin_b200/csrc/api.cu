@@ -79,6 +79,7 @@ DomainView ahx::view_at(ahx_handle* h, int parity) {
   D.ps = h->ps;
   D.qs = h->qs;
   set_offsets(D);
+  set_pointers(D, h->esize, h->esize_g);
   return D;
 }
 
@@ -870,6 +871,7 @@ ahx_status ahx_autotune(ahx_handle* h, int steps_per_trial, int* best_block_y, i
           D.fB = (s & 1) ? f0 : f1;
           D.gA = (s & 1) ? g1 : g0;
           D.gB = (s & 1) ? g0 : g1;
+          set_pointers(D, h->esize, h->esize_g);
           L.maps = sh.ty ? &tm[sh.ty == 8 ? 1 : 0][s & 1] : nullptr;
           const cudaError_t e = h->dims.arith == AHX_ARITH_FAST ? fast::launch_step(D, L, h->s_step)
                                                                   : exact::launch_step(D, L, h->s_step);

@@ -315,11 +315,11 @@ __device__ __forceinline__ void stream_interior(const DomainView& D, const float
   X.kb = R(pr.z);
   static_for<19>([&](auto Q) {
     constexpr int q = Q;
-    X.f[q] = KF::dec_f(KF::load(fA + (n + D.pull_f[q])), R(w19(q)));
+    X.f[q] = KF::dec_f(KF::load(static_cast<const StoreF<S>*>(D.src_f[q]) + n), R(w19(q)));
   });
   static_for<7>([&](auto Q) {
     constexpr int q = Q;
-    X.g[q] = KG::dec_g(KG::load(gA + (n + D.pull_g[q])));
+    X.g[q] = KG::dec_g(KG::load(static_cast<const StoreG<S>*>(D.src_g[q]) + n));
   });
 }
 
@@ -498,11 +498,11 @@ __device__ __forceinline__ void fast_update(const DomainView& D, const ParamsHea
       P, m, X.g, X.uI, X.vI, X.kb, sg, Fx0, Fy0, Ssrc, tb_add, o,
       [&](auto Q, R v) {
         constexpr int q = Q;
-        KF::store(fB + (q == 0 ? n : n + D.plane[q]), KF::enc_f(v, R(w19(q))));
+        KF::store(static_cast<StoreF<S>*>(D.dst_f[q]) + n, KF::enc_f(v, R(w19(q))));
       },
       [&](auto Q, R v) {
         constexpr int q = Q;
-        KG::store(gB + (q == 0 ? n : n + D.plane[q]), KG::enc_g(v));
+        KG::store(static_cast<StoreG<S>*>(D.dst_g[q]) + n, KG::enc_g(v));
       });
   M.rho = m.rho;
   M.jx = m.jx;
@@ -574,11 +574,11 @@ __device__ __forceinline__ void fast_pair(const DomainView& D, const ParamsHead&
   float2 f[19], g[7];
   static_for<19>([&](auto Q) {
     constexpr int q = Q;
-    f[q] = pair_load_f(fA + (n + D.pull_f[q]), ps, (float)w19(q));
+    f[q] = pair_load_f(static_cast<const StoreF<S>*>(D.src_f[q]) + n, ps, (float)w19(q));
   });
   static_for<7>([&](auto Q) {
     constexpr int q = Q;
-    g[q] = pair_load_g(gA + (n + D.pull_g[q]), ps);
+    g[q] = pair_load_g(static_cast<const StoreG<S>*>(D.src_g[q]) + n, ps);
   });
   const int z0 = min(max(k - C.ktc, 0), D.nz - 1), z1 = min(max(k + 1 - C.ktc, 0), D.nz - 1);
   const float4 p0 = prof[z0], p1 = prof[z1];
@@ -592,11 +592,11 @@ __device__ __forceinline__ void fast_pair(const DomainView& D, const ParamsHead&
       make_float2(sponge_sg(P, D.nz, k), sponge_sg(P, D.nz, k + 1)), zero, zero, zero, tb_add, o,
       [&](auto Q, float2 v) {
         constexpr int q = Q;
-        pair_store_f(fB + (q == 0 ? n : n + D.plane[q]), ps, v, (float)w19(q));
+        pair_store_f(static_cast<StoreF<S>*>(D.dst_f[q]) + n, ps, v, (float)w19(q));
       },
       [&](auto Q, float2 v) {
         constexpr int q = Q;
-        pair_store_g(gB + (q == 0 ? n : n + D.plane[q]), ps, v);
+        pair_store_g(static_cast<StoreG<S>*>(D.dst_g[q]) + n, ps, v);
       });
 }
 

@@ -33,6 +33,9 @@ __device__ __forceinline__ float2 vmul(float2 a, float2 b) { return __fmul2_rn(a
 __device__ __forceinline__ float2 vadd(float2 a, float2 b) { return __fadd2_rn(a, b); }
 __device__ __forceinline__ float2 vsub(float2 a, float2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
 __device__ __forceinline__ float2 vrcp(float2 a) { return make_float2(vrcp(a.x), vrcp(a.y)); }
+__device__ __forceinline__ float vneg(float a) { return -a; }
+__device__ __forceinline__ double vneg(double a) { return -a; }
+__device__ __forceinline__ float2 vneg(float2 a) { return make_float2(-a.x, -a.y); }
 __device__ __forceinline__ float2 vsqrt(float2 a) { return make_float2(vsqrt(a.x), vsqrt(a.y)); }
 
 // a constant in lane type V
@@ -51,7 +54,7 @@ __device__ __forceinline__ V vdot(V a, V b, V c) {
   V acc = vc<V>(0.0);
   bool first = true;
   auto term = [&](V x, int s) {
-    if (first) acc = s > 0 ? x : vsub(vc<V>(0.0), x);
+    if (first) acc = s > 0 ? x : vneg(x);
     else acc = s > 0 ? vadd(acc, x) : vsub(acc, x);
     first = false;
   };
@@ -130,20 +133,20 @@ __device__ __forceinline__ void lane_relax(const ParamsHead& P, const Moments<V>
                                            PutG&& put_g) {
   const V rho = m.rho, irho = m.irho, jx = m.jx, jy = m.jy, jz = m.jz;
   const V rs = vmul(rho, sg);
-  const V Fx = vfma(rs, vsub(uI, vmul(jx, irho)), Fx0);
-  const V Fy = vfma(rs, vsub(vI, vmul(jy, irho)), Fy0);
-  const V Fz = vsub(vmul(vmul(rho, vc<V>(P.gbeta)), m.th), vmul(rs, vmul(jz, irho)));
+  const V Fx = vfma(rs, vfma(vneg(jx), irho, uI), Fx0);
+  const V Fy = vfma(rs, vfma(vneg(jy), irho, vI), Fy0);
+  const V Fz = vfma(vneg(rs), vmul(jz, irho), vmul(vmul(rho, vc<V>(P.gbeta)), m.th));
   const V half = vc<V>(0.5);
   const V ux = vmul(vfma(half, Fx, jx), irho), uy = vmul(vfma(half, Fy, jy), irho), uz = vmul(vfma(half, Fz, jz), irho);
   const V usq = vfma(uz, uz, vfma(uy, uy, vmul(ux, ux)));
   const V r3 = vmul(rho, vc<V>(1.0 / 3.0));
   const V rux = vmul(rho, ux), ruy = vmul(rho, uy), ruz = vmul(rho, uz);
-  const V Nxx = vsub(vsub(m.Pxx, r3), vmul(rux, ux));
-  const V Nyy = vsub(vsub(m.Pyy, r3), vmul(ruy, uy));
-  const V Nzz = vsub(vsub(m.Pzz, r3), vmul(ruz, uz));
-  const V Nxy = vsub(m.Pxy, vmul(rux, uy));
-  const V Nxz = vsub(m.Pxz, vmul(rux, uz));
-  const V Nyz = vsub(m.Pyz, vmul(ruy, uz));
+  const V Nxx = vfma(vneg(rux), ux, vsub(m.Pxx, r3));
+  const V Nyy = vfma(vneg(ruy), uy, vsub(m.Pyy, r3));
+  const V Nzz = vfma(vneg(ruz), uz, vsub(m.Pzz, r3));
+  const V Nxy = vfma(vneg(rux), uy, m.Pxy);
+  const V Nxz = vfma(vneg(rux), uz, m.Pxz);
+  const V Nyz = vfma(vneg(ruy), uz, m.Pyz);
   const V off2 = vfma(Nyz, Nyz, vfma(Nxz, Nxz, vmul(Nxy, Nxy)));
   const V Pn = vsqrt(vfma(vc<V>(2.0), off2, vfma(Nzz, Nzz, vfma(Nyy, Nyy, vmul(Nxx, Nxx)))));
   const V tb = vadd(vfma(vc<V>(3.0 * P.momfac), kb, vc<V>(P.tau0)), tb_add);
@@ -153,10 +156,10 @@ __device__ __forceinline__ void lane_relax(const ParamsHead& P, const Moments<V>
   const V kap = vadd(vfma(nusgs, vc<V>(1.0 / P.prt), kb), vc<V>(P.kfloor));
   const V taug = vfma(vc<V>(4.0), kap, half);
   const V om = vsub(vc<V>(1.0), itau);
-  const V fpre = vsub(vc<V>(1.0), vmul(half, itau));
+  const V fpre = vfma(vc<V>(-0.5), itau, vc<V>(1.0));
   const V trN = vmul(vadd(vadd(Nxx, Nyy), Nzz), vc<V>(1.0 / 3.0));
   const V uF = vfma(uz, Fz, vfma(uy, Fy, vmul(ux, Fx)));
-  const V base = vsub(vc<V>(1.0), vmul(vc<V>(1.5), usq));
+  const V base = vfma(vc<V>(-1.5), usq, vc<V>(1.0));
   const V m3uF = vmul(vc<V>(-3.0), uF);
   const V omtr = vmul(om, trN);
   {
@@ -185,7 +188,7 @@ __device__ __forceinline__ void lane_relax(const ParamsHead& P, const Moments<V>
     if constexpr (cy != 0 && cz != 0) qn = vfma(vc<V>(2 * cy * cz), Nyz, qn);
     // even part: w [rho (base + 4.5 cu^2) + 4.5 om (qn - trN) + fpre (9 cu cF - 3 uF)]
     const V ev = vfma(fpre, vfma(vmul(vc<V>(9.0), cu), cF, m3uF),
-                      vfma(vc<V>(4.5), vsub(vmul(om, qn), omtr), vmul(rho, vfma(vmul(vc<V>(4.5), cu), cu, base))));
+                      vfma(vc<V>(4.5), vfma(om, qn, vneg(omtr)), vmul(rho, vfma(vmul(vc<V>(4.5), cu), cu, base))));
     // odd part: 3 w (rho cu + fpre cF)
     const V od = vmul(vc<V>(3.0), vfma(fpre, cF, vmul(rho, cu)));
     put_f(std::integral_constant<int, q>{}, vmul(w, vadd(ev, od)));

@@ -193,6 +193,12 @@ struct DomainView {
   // (kernel-parameter table, so each gather is one add of a constant operand)
   uint32_t pull_f[19], pull_g[7];
   uint32_t plane[19];           // q*qs
+  // interior accesses as (base pointer + cell index): the pull source of each population (fA / gA + pull offset) and
+  // each population plane of the next state (fB / gB + q*qs), filled by set_pointers
+  const void* src_f[19];
+  const void* src_g[7];
+  void* dst_f[19];
+  void* dst_g[7];
 };
 
 // fill the offset tables of a view from its strides
@@ -203,6 +209,19 @@ inline void set_offsets(DomainView& D) {   // host only
   }
   for (int q = 0; q < 7; ++q)
     D.pull_g[q] = (uint32_t)q * D.qs - (uint32_t)(kC7[q][0] + kC7[q][1] * D.px + kC7[q][2] * (int)D.ps);
+}
+
+// fill the interior base pointers of a view from its state pointers and offset tables (host only; call again when
+// fA / fB / gA / gB change)
+inline void set_pointers(DomainView& D, int esize_f, int esize_g) {
+  for (int q = 0; q < 19; ++q) {
+    D.src_f[q] = static_cast<const unsigned char*>(D.fA) + (size_t)D.pull_f[q] * esize_f;
+    D.dst_f[q] = static_cast<unsigned char*>(D.fB) + (size_t)D.plane[q] * esize_f;
+  }
+  for (int q = 0; q < 7; ++q) {
+    D.src_g[q] = static_cast<const unsigned char*>(D.gA) + (size_t)D.pull_g[q] * esize_g;
+    D.dst_g[q] = static_cast<unsigned char*>(D.gB) + (size_t)D.plane[q] * esize_g;
+  }
 }
 
 }  // namespace ahx
