@@ -30,6 +30,8 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+from ashburn_heat_twin_b200 import replicas as RP  # noqa: E402
+
 WORKLOADS = {
     'c2': dict(desc='600x600x64 cells at 10 m (23.04 M), synthetic seed 2: 24 hills 0-40 m, 4000 buildings, '
                     '211 DC roofs', dx=10, heightM=640, met='C2_MET', spec='C2'),
@@ -228,9 +230,7 @@ def main_batch(a, rank, world, local, dist, torch):
     b._b.time_steps(a.warmup)
 
     def barrier():
-        if dist is not None:
-            dist.barrier()
-        torch.cuda.synchronize(local)
+        RP.barrier(dist, lambda: torch.cuda.synchronize(local))
 
     barrier()
     with Clocks(local) as clk:
@@ -238,12 +238,8 @@ def main_batch(a, rank, world, local, dist, torch):
         ms = b._b.time_steps(a.steps)
         barrier()
     clocks = clk.summary()
-    ms_all = ms
-    if dist is not None:
-        t = torch.tensor([ms], device=f'cuda:{local}', dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_all = float(t.item())
-    value = world * cells * a.steps / (ms_all / 1e3) / 1e9
+    ms_all = RP.max_over_ranks(ms, dist, f'cuda:{local}')
+    value = RP.aggregate_rate(cells * a.steps, world, ms_all / 1e3) / 1e9
     # the same members stepped one after another with their own tuned launches (no batch)
     serial_ms = sum(s._dev.time_steps(a.steps) for s in solvers)
     bytes_launch = fluid * CELL_BYTES[a.precision]
@@ -272,11 +268,7 @@ def main_batch(a, rank, world, local, dist, torch):
             p.result()
             d2h += 3 * s.info['nx'] * s.info['ny'] * 4 + 4
     barrier()
-    e2e_s = time.perf_counter() - t0
-    if dist is not None:
-        t = torch.tensor([e2e_s], device=f'cuda:{local}', dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = RP.max_over_ranks(time.perf_counter() - t0, dist, f'cuda:{local}')
     e2e = dict(value=world * cells * F * frames / e2e_s / 1e9, unit='GLUPS', h2d_bytes_per_step=h2d / (F * frames),
                d2h_bytes_per_step=d2h / (F * frames), frame_steps=F, frames=frames,
                per_frame='setMet on all 64 members (parameter blocks H2D) + batch step(F) + read(wind) of every member '
@@ -516,9 +508,7 @@ def main():
     a = ap.parse_args()
     a.warmup = max(a.warmup, 3)
 
-    rank = int(os.environ.get('RANK', '0'))
-    world = int(os.environ.get('WORLD_SIZE', '1'))
-    local = int(os.environ.get('LOCAL_RANK', '0'))
+    rank, world, local = RP.env_ranks()
     if a.impl == 'reference':
         return run_reference(a, rank)
 
@@ -554,9 +544,7 @@ def main():
     dev.time_steps(a.warmup)
 
     def barrier():
-        if dist is not None:
-            dist.barrier()
-        torch.cuda.synchronize(local)
+        RP.barrier(dist, lambda: torch.cuda.synchronize(local))
 
     barrier()
     with Clocks(local) as clk:
@@ -564,12 +552,8 @@ def main():
         ms = dev.time_steps(a.steps)
         barrier()
     clocks = clk.summary()
-    ms_all = ms
-    if dist is not None:
-        t = torch.tensor([ms], device=f'cuda:{local}', dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_all = float(t.item())
-    value = world * cells * a.steps / (ms_all / 1e3) / 1e9
+    ms_all = RP.max_over_ranks(ms, dist, f'cuda:{local}')
+    value = RP.aggregate_rate(cells * a.steps, world, ms_all / 1e3) / 1e9
 
     # roofline of the step kernel (one launch per step): algorithmic bytes = fluid cells x (read + write of 19 f and
     # 7 g populations) at the storage width
@@ -602,11 +586,7 @@ def main():
     for p in pend:
         p.result()
     barrier()
-    e2e_s = time.perf_counter() - t0
-    if dist is not None:
-        t = torch.tensor([e2e_s], device=f'cuda:{local}', dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = RP.max_over_ranks(time.perf_counter() - t0, dist, f'cuda:{local}')
     NXY = nx * ny
     h2d = len(s._params)
     d2h = 3 * NXY * 4 + s.nzv * NXY + 4
