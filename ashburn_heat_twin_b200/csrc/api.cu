@@ -71,6 +71,8 @@ DomainView ahx::view_at(ahx_handle* h, int parity) {
   D.gB = h->g[1 - parity];
   D.dbg = h->d_dbg;
   D.budget = h->d_budget;
+  D.sacc = h->accum_on ? h->d_sacc : nullptr;
+  D.facc = h->accum_on ? h->d_facc : nullptr;
   D.err = h->d_err;
   D.nx = h->dims.nx;
   D.ny = h->dims.ny;
@@ -185,7 +187,8 @@ void free_all(ahx_handle* h) {
     if (h->g[p]) cudaFree(h->g[p]);
     h->f[p] = h->g[p] = nullptr;
   }
-  void* devs[] = {h->d_params, h->d_colv, h->d_ktop, h->d_oldk, h->d_dbg, h->d_budget, h->d_stats, h->d_err};
+  void* devs[] = {h->d_params, h->d_colv, h->d_ktop, h->d_oldk, h->d_dbg, h->d_budget, h->d_stats, h->d_err,
+                  h->d_sacc, h->d_facc};
   for (void* p : devs)
     if (p) cudaFree(p);
   h->d_params = nullptr;
@@ -193,6 +196,7 @@ void free_all(ahx_handle* h) {
   h->d_ktop = h->d_oldk = nullptr;
   h->d_dbg = nullptr;
   h->d_budget = nullptr;
+  h->d_sacc = h->d_facc = nullptr;
   h->d_stats = nullptr;
   h->d_err = nullptr;
   for (auto& r : h->reads) {
@@ -442,7 +446,7 @@ ahx_status ahx_step(ahx_handle* h, int n, int mode) {
     if (ahx_status st = ensure_dbg(h)) return st;
   StepLaunch L;
   L.precision = h->dims.precision;
-  L.budget = h->budget_on;
+  L.budget = h->budget_on || h->accum_on;
   L.block_y = h->block_y;
   L.zslab = h->zslab;
   L.minb = h->minb;
@@ -458,6 +462,7 @@ ahx_status ahx_step(ahx_handle* h, int n, int mode) {
     if (e != cudaSuccess) return cuda_fail(h, e, "step launch");
     h->parity ^= 1;
     ++h->steps;
+    if (h->accum_on) ++h->accum_steps;
   }
   return AHX_OK;
 }
@@ -761,6 +766,52 @@ ahx_status ahx_budget_read(ahx_handle* h, ahx_budget_out* out, int reset) {
     out->face_u[a] = acc[6 + a];
   }
   out->cells = acc[10];
+  return AHX_OK;
+}
+
+size_t face_doubles(const ahx_handle* h) {
+  return 2 * (2 * (size_t)h->dims.ny * h->dims.nz + 2 * (size_t)h->dims.nx * h->dims.nz);
+}
+
+ahx_status ahx_accum_enable(ahx_handle* h, int on) {
+  if (!h) return fail(AHX_EINVAL, "live solver: null handle");
+  std::lock_guard<std::mutex> lk(h->mu);
+  if (ahx_status st = check(h)) return st;
+  AHX_CUDA(h, cudaSetDevice(h->dev));
+  if (on && !h->d_sacc) {
+    if (cudaMalloc(&h->d_sacc, 3 * nxy(h) * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&h->d_facc, face_doubles(h) * sizeof(double)) != cudaSuccess) {
+      cudaGetLastError();
+      if (h->d_sacc) cudaFree(h->d_sacc);
+      h->d_sacc = nullptr;
+      return fail(AHX_ENOMEM, "live solver: accumulator allocation failed");
+    }
+    AHX_CUDA(h, cudaMemsetAsync(h->d_sacc, 0, 3 * nxy(h) * sizeof(double), h->s_step));
+    AHX_CUDA(h, cudaMemsetAsync(h->d_facc, 0, face_doubles(h) * sizeof(double), h->s_step));
+    h->accum_steps = 0;
+  }
+  h->accum_on = on != 0;
+  return AHX_OK;
+}
+
+ahx_status ahx_accum_read(ahx_handle* h, double* surf3, double* faces, int64_t* steps, int reset) {
+  if (!h) return fail(AHX_EINVAL, "live solver: null handle");
+  std::lock_guard<std::mutex> lk(h->mu);
+  if (ahx_status st = check(h)) return st;
+  if (!h->d_sacc) return fail(AHX_EINVAL, "live solver: accumulators were never enabled");
+  AHX_CUDA(h, cudaSetDevice(h->dev));
+  if (surf3)
+    AHX_CUDA(h, cudaMemcpyAsync(surf3, h->d_sacc, 3 * nxy(h) * sizeof(double), cudaMemcpyDeviceToHost, h->s_step));
+  if (faces)
+    AHX_CUDA(h, cudaMemcpyAsync(faces, h->d_facc, face_doubles(h) * sizeof(double), cudaMemcpyDeviceToHost,
+                                h->s_step));
+  if (reset) {
+    AHX_CUDA(h, cudaMemsetAsync(h->d_sacc, 0, 3 * nxy(h) * sizeof(double), h->s_step));
+    AHX_CUDA(h, cudaMemsetAsync(h->d_facc, 0, face_doubles(h) * sizeof(double), h->s_step));
+  }
+  AHX_CUDA(h, cudaStreamSynchronize(h->s_step));
+  if (steps) *steps = h->accum_steps;
+  if (reset) h->accum_steps = 0;
   return AHX_OK;
 }
 

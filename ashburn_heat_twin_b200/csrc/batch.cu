@@ -454,8 +454,9 @@ ahx_status ahx_batch_step(ahx_batch* b, int n) {
   for (size_t m = 0; m < M; ++m) {
     ahx_handle* h = b->members[m];
     if (ahx_status st = check(h)) return st;
-    if (h->budget_on) return fail(AHX_EINVAL, "live solver: batched steps do not accumulate budgets (member " +
-                                                  std::to_string(m) + " has them enabled)");
+    if (h->budget_on || h->accum_on)
+      return fail(AHX_EINVAL, "live solver: batched steps do not accumulate budgets or time sums (member " +
+                                  std::to_string(m) + " has them enabled)");
     if (h->parity != (b->base_parity[m] ^ b->phase)) moved = true;   // stepped on its own since
   }
   if (moved)

@@ -695,6 +695,21 @@ __device__ __forceinline__ void step_block(const DomainView& D, int bx, int by, 
         if (C.latE) { B.ftu[1] += th * ux; B.fu[1] += ux; }
         if (C.latS) { B.ftu[2] += th * uy; B.fu[2] += uy; }
         if (C.latN) { B.ftu[3] += th * uy; B.fu[3] += uy; }
+        // time accumulators: one thread owns each column and each face cell, so plain read-modify-writes suffice
+        if (D.sacc != nullptr && k == C.kg) {
+          double* a = D.sacc + 3 * ((size_t)j * D.nx + i);
+          a[0] += (double)th;
+          a[1] += (double)ux;
+          a[2] += (double)uy;
+        }
+        if (D.facc != nullptr && C.face) {
+          const size_t fy = (size_t)D.ny * D.nz, fx = (size_t)D.nx * D.nz;
+          const size_t cy = (size_t)k * D.ny + j, cx = (size_t)k * D.nx + i;
+          if (C.latW) { D.facc[2 * cy] += (double)th; D.facc[2 * cy + 1] += (double)ux; }
+          if (C.latE) { D.facc[2 * (fy + cy)] += (double)th; D.facc[2 * (fy + cy) + 1] += (double)ux; }
+          if (C.latS) { D.facc[2 * (2 * fy + cx)] += (double)th; D.facc[2 * (2 * fy + cx) + 1] += (double)uy; }
+          if (C.latN) { D.facc[2 * (2 * fy + fx + cx)] += (double)th; D.facc[2 * (2 * fy + fx + cx) + 1] += (double)uy; }
+        }
       }
     }
   }

@@ -64,6 +64,10 @@ struct ahx_handle {
   float4* d_dbg = nullptr;
   double* d_budget = nullptr;
   bool budget_on = false;
+  bool accum_on = false;                  // FP64 time accumulators (near-ground and lateral faces)
+  double* d_sacc = nullptr;               // 3 * NXY
+  double* d_facc = nullptr;               // 2 * (2 ny nz + 2 nx nz)
+  int64_t accum_steps = 0;
   ahx::StatsScratch* d_stats = nullptr;
   int parity = 0;
   int64_t steps = 0;

@@ -185,6 +185,10 @@ struct DomainView {
   void* gB;
   float4* dbg;                  // (theta, ux, uy, uz) per cell (pitched), or null
   double* budget;               // per-step FP64 budget accumulators, or null
+  // FP64 time accumulators (budget variant only), or null: per column at the first fluid cell (theta, ux, uy);
+  // per lateral-face cell (theta, u_n): west / east [k][j], then south / north [k][i]
+  double* sacc;
+  double* facc;
   int* err;                     // error word: a staged copy that did not arrive in time sets it
   int nx, ny, nz, px;
   uint32_t ps;                  // plane stride px*ny

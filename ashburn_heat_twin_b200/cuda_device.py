@@ -26,7 +26,7 @@ SYMBOLS = ('ahx_create', 'ahx_destroy', 'ahx_last_error', 'ahx_get_info', 'ahx_s
            'ahx_read_state_f64', 'ahx_write_state_f64', 'ahx_read_dbg', 'ahx_clear_dbg', 'ahx_stats',
            'ahx_budget_enable', 'ahx_budget_read', 'ahx_set_launch', 'ahx_autotune', 'ahx_time_steps', 'ahx_stats_noalloc',
            'ahx_batch_create', 'ahx_batch_step', 'ahx_batch_time_steps', 'ahx_batch_sync', 'ahx_batch_set_launch',
-           'ahx_batch_get_info', 'ahx_batch_destroy', 'ahx_batch_set_members')
+           'ahx_batch_get_info', 'ahx_batch_destroy', 'ahx_batch_set_members', 'ahx_accum_enable', 'ahx_accum_read')
 
 
 class AhxError(RuntimeError):
@@ -114,6 +114,8 @@ def load_library(path: str = LIB_PATH):
         'ahx_batch_sync': [H, i],
         'ahx_batch_set_launch': [H, i, i, i, i],
         'ahx_batch_set_members': [H, ctypes.POINTER(H), i],
+        'ahx_accum_enable': [H, i],
+        'ahx_accum_read': [H, vp, vp, ctypes.POINTER(ctypes.c_int64), i],
         'ahx_batch_get_info': [H, ctypes.POINTER(BatchInfoOut)],
         'ahx_batch_destroy': [H],
     }
@@ -333,6 +335,24 @@ class CudaDevice:
 
     def set_launch(self, block_y=0, zslab=0):
         self._c('ahx_set_launch', int(block_y), int(zslab))
+
+    def accum_enable(self, on=True):
+        self._c('ahx_accum_enable', int(bool(on)))
+
+    def accum_read(self, reset=False):
+        """FP64 sums since enable / last reset: surf (3, ny, nx) = theta, ux, uy at the first fluid cell (solver
+        orientation, lattice units), faces = dict(west, east: (2, nz, ny); south, north: (2, nz, nx)) of
+        (theta, u_n), and the number of steps."""
+        nx, ny, nz = self.nx, self.ny, self.nz
+        surf = np.empty(3 * nx * ny, np.float64)
+        faces = np.empty(2 * (2 * ny * nz + 2 * nx * nz), np.float64)
+        n = ctypes.c_int64()
+        self._c('ahx_accum_read', _ptr(surf), _ptr(faces), ctypes.byref(n), int(bool(reset)))
+        fy, fx = ny * nz, nx * nz
+        fc = faces.reshape(-1, 2)
+        out = dict(west=fc[:fy], east=fc[fy:2 * fy], south=fc[2 * fy:2 * fy + fx], north=fc[2 * fy + fx:])
+        out = {k: v.T.reshape(2, nz, -1) for k, v in out.items()}
+        return surf.reshape(ny, nx, 3).transpose(2, 0, 1), out, n.value
 
     def autotune(self, steps_per_trial=4):
         by, zs, ms = ctypes.c_int(), ctypes.c_int(), ctypes.c_float()

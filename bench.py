@@ -391,8 +391,8 @@ def main_serve(a, rank, world, local, dist, torch):
 
 def main_precision(a, rank, world, local, dist, torch):
     """Storage precision study on the 600x600x64 domain: every storage (FP32, FP16, BF16 with the FMA build; FP64 with
-    the exact build) runs the same cold start for --spin-s simulated seconds, then accumulates the --mean-s mean of
-    theta with the FP64 heat budget fused into the step. Reported per storage against FP64: rel-L2 of the mean
+    the exact build) runs the same cold start for --spin-s simulated seconds, then takes the --mean-s time means with
+    the FP64 heat budget and the FP64 near-ground / lateral-face accumulators fused into the step. Reported per storage against FP64: rel-L2 of the mean
     near-ground theta (the first fluid cell of every column), peak mean warming, heat-closure terms, the rel-L2 of
     theta after one step from the FP64 state, and the step rate (GLUPS) on the tuned launch."""
     import numpy as np
@@ -408,7 +408,6 @@ def main_precision(a, rank, world, local, dist, torch):
     mean = int(round(a.mean_s / dt))
     ktop = s0._ktopS.astype(np.int64)            # solver orientation, j = 0 south
     cols = np.nonzero(ktop < nz)[0]
-    first = ktop[cols] * (nx * ny) + cols        # reference-layout index of each column's first fluid cell
     fluid = (np.arange(nz)[:, None] >= ktop[None, :]).reshape(-1)
     res = {}
     for p in order:
@@ -419,17 +418,23 @@ def main_precision(a, rank, world, local, dist, torch):
         st0 = dev.stats()
         dev.budget_enable(True)
         dev.budget_read(reset=True)
-        s._dbg.clearDbg()
-        s._dbg.stepAcc(mean).result()
+        dev.accum_enable(True)
+        dev.accum_read(reset=True)
+        s.step(mean).result()
         bud = dev.budget_read(reset=True)
+        surf, faces, nacc = dev.accum_read(reset=True)
         dev.budget_enable(False)
+        dev.accum_enable(False)
         st1 = dev.stats()
-        dbg = s._dbg.readDbg().reshape(N, 4)
-        ng = dbg[first, 0].astype(np.float64) / mean
+        ng = surf[0].reshape(-1)[cols] / nacc                   # mean theta at each column's first fluid cell
         rc = PM.RHO_CP * dx ** 3 / (mean * dt) / 1e6          # K lattice units summed over the window -> MW
         ftu = bud['face_theta_u']                              # west, east, south, north sums of theta * u_n
         out_mw = rc * (ftu[1] - ftu[0] + ftu[3] - ftu[2])
+        # the offline form (product of the time means on the faces)
+        pm = {k: float((v[0] / nacc * v[1] / nacc).sum()) for k, v in faces.items()}
+        out_pm_mw = PM.RHO_CP * dx ** 3 / dt / 1e6 * (pm['east'] - pm['west'] + pm['north'] - pm['south'])
         res[p] = dict(ng=ng, peak=float(ng.max()), injected_mw=rc * bud['src_sum'], advected_out_mw=out_mw,
+                      advected_out_mean_product_mw=out_pm_mw,
                       content_rate_mw=rc * (st1['sumTheta'] - st0['sumTheta']), nonfinite=st1['nonFinite'],
                       wall_s=time.perf_counter() - t0)
         log(f'[rank {rank}] precision {p}: {spin}+{mean} steps in {res[p]["wall_s"]:.1f} s, peak {res[p]["peak"]:.4f} K')
@@ -466,6 +471,7 @@ def main_precision(a, rank, world, local, dist, torch):
                        mean_ng_theta_rel_l2_vs_fp64=None if p == 'fp64' else rel_l2(r['ng'], ref['ng']),
                        step_theta_rel_l2_vs_fp64=step_err.get(p), peak_mean_warming_k=r['peak'],
                        injected_mw=r['injected_mw'], advected_out_mw=r['advected_out_mw'],
+                       advected_out_product_of_means_mw=r['advected_out_mean_product_mw'],
                        content_rate_mw=r['content_rate_mw'], closure_residual_frac=closure,
                        nonfinite=r['nonfinite'])
     out = dict(metric='GLUPS (all cells) of the FP16-storage step on 600x600x64, with its 10-minute mean near-ground '

@@ -186,6 +186,15 @@ ahx_status ahx_stats(ahx_handle* h, ahx_stats_out* out);               /* synchr
 ahx_status ahx_budget_enable(ahx_handle* h, int on);
 ahx_status ahx_budget_read(ahx_handle* h, ahx_budget_out* out, int reset);
 
+/* Time accumulators, no counterpart in the reference (it takes its time means offline from the +32 B/cell
+ * accumulate mode, tools/live/validate_live.py:226-255). While enabled, every step adds, in FP64: per column at its
+ * first fluid cell (theta, ux, uy) in lattice units, solver orientation [j][i] (j = 0 south); per lateral-face cell
+ * (theta, u_n): west then east faces as [k][j], then south then north faces as [k][i]. Enabling allocates and zeroes
+ * them; ahx_accum_read copies the sums (surf3: 3 * nx * ny doubles; faces: 2 * (2 ny nz + 2 nx nz) doubles; either may
+ * be NULL) and the number of steps accumulated, optionally resetting both (synchronous). */
+ahx_status ahx_accum_enable(ahx_handle* h, int on);
+ahx_status ahx_accum_read(ahx_handle* h, double* surf3, double* faces, int64_t* steps, int reset);
+
 /* --- tuning ----------------------------------------------------------------------------------------------------- */
 
 /* launch shape of the fused step: block_y = threads per block in y (x is one warp) plus 100 x the register-budget
@@ -221,8 +230,8 @@ ahx_status ahx_stats_noalloc(int nx, int ny, int nz, const float* f, const float
  * (a member's result is bit-identical to stepping it alone), replayed two steps at a time from a CUDA graph. Members
  * stay usable on their own (parameters, columns, reads, solo steps): the batch's launches are ordered after the work
  * already queued on each member's stream and before anything queued there later. A member cannot be destroyed while
- * it belongs to a batch (AHX_EINVAL), and batched steps do not accumulate budgets (members with budgets enabled are
- * rejected). Tiles are 32 x 4 columns x 8 levels, handed to the persistent blocks from a device counter in list order;
+ * it belongs to a batch (AHX_EINVAL), and batched steps do not accumulate budgets or time sums (members with either
+ * enabled are rejected). Tiles are 32 x 4 columns x 8 levels, handed to the persistent blocks from a device counter in list order;
  * the register-budget variant is the members' tuned one when they agree, else 4. ahx_batch_set_launch overrides
  * both. */
 typedef struct ahx_batch ahx_batch;

@@ -247,3 +247,43 @@ def test_f32_g_storage_keeps_the_heat_content():
     e16 = abs(runs['fp16'] / runs['fp64'] - 1)
     e32 = abs(runs['fp16g32'] / runs['fp64'] - 1)
     assert e32 < e16 and e32 < 1e-4, (e16, e32)
+
+
+def test_time_accumulators_equal_host_sums_of_step_outputs():
+    """ahx_accum_*: FP64 sums over steps of (theta, ux, uy) at each column's first fluid cell and of (theta, u_n) on
+    the lateral faces equal the same sums taken on the host over the per-step out-mode fields (same floats, same
+    order)."""
+    met = dict(u10=5.0, dirFrom=250.0, wstar=1.5, blh=700.0)
+    g = small_solver(cuda_backend('fp32', 'fast'), met=met)
+    g.step(10).result()
+    nx, ny, nz = g.info['nx'], g.info['ny'], g.info['nz']
+    ktop = g._ktopS.reshape(ny, nx).astype(np.int64)
+    g._dev.accum_enable(True)
+    hs = np.zeros((3, ny, nx))
+    hf = dict(west=np.zeros((2, nz, ny)), east=np.zeros((2, nz, ny)), south=np.zeros((2, nz, nx)),
+              north=np.zeros((2, nz, nx)))
+    jj, ii = np.meshgrid(np.arange(ny), np.arange(nx), indexing='ij')
+    kk = np.arange(nz)[:, None]
+    for _ in range(12):
+        g._dbg.stepOut(1).result()
+        d = g._dbg.readDbg().reshape(nz, ny, nx, 4).astype(np.float64)
+        fl = ktop < nz
+        for c, comp in enumerate((0, 1, 2)):
+            v = d[np.minimum(ktop, nz - 1), jj, ii, comp]
+            hs[c] += np.where(fl, v, 0.0)
+        for name, sl, comp, kt in (('west', (slice(None), slice(None), 0), 1, ktop[:, 0]),
+                                   ('east', (slice(None), slice(None), nx - 1), 1, ktop[:, nx - 1]),
+                                   ('south', (slice(None), 0, slice(None)), 2, ktop[0, :]),
+                                   ('north', (slice(None), ny - 1, slice(None)), 2, ktop[ny - 1, :])):
+            plane = d[sl]                                   # (nz, n, 4)
+            m = kk >= kt[None, :]
+            hf[name][0] += np.where(m, plane[:, :, 0], 0.0)
+            hf[name][1] += np.where(m, plane[:, :, comp], 0.0)
+    surf, faces, n = g._dev.accum_read(reset=True)
+    assert n == 12
+    assert np.array_equal(surf, hs)
+    for name in hf:
+        assert np.array_equal(faces[name], hf[name]), name
+    surf2, _, n2 = g._dev.accum_read()
+    assert n2 == 0 and not surf2.any()
+    g.destroy()
