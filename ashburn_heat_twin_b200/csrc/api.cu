@@ -78,6 +78,11 @@ DomainView ahx::view_at(ahx_handle* h, int parity) {
   D.ny = h->dims.ny;
   D.nz = h->dims.nz;
   D.px = h->px;
+  const bool slab = h->nyg > 0;
+  D.jg0 = slab ? h->jg0 : 0;
+  D.nyg = slab ? h->nyg : h->dims.ny;
+  D.jlo = slab ? h->jlo : 0;
+  D.jhi = slab ? h->jhi : h->dims.ny;
   D.ps = h->ps;
   D.qs = h->qs;
   set_offsets(D);
@@ -813,6 +818,49 @@ ahx_status ahx_accum_read(ahx_handle* h, double* surf3, double* faces, int64_t* 
   if (steps) *steps = h->accum_steps;
   if (reset) h->accum_steps = 0;
   return AHX_OK;
+}
+
+ahx_status ahx_set_slab(ahx_handle* h, int jg0, int nyg, int jlo, int jhi) {
+  if (!h) return fail(AHX_EINVAL, "live solver: null handle");
+  std::lock_guard<std::mutex> lk(h->mu);
+  if (ahx_status st = check(h)) return st;
+  const int ny = h->dims.ny;
+  if (nyg < ny || jg0 < 0 || jg0 + ny > nyg || jlo < 0 || jhi > ny || jlo >= jhi)
+    return fail(AHX_EINVAL, "live solver: bad slab (need 0 <= jg0, jg0 + ny <= nyg, 0 <= jlo < jhi <= ny)");
+  if (h->batch_refs > 0) return fail(AHX_EINVAL, "live solver: a batch member cannot become a slab");
+  h->jg0 = jg0;
+  h->nyg = nyg;
+  h->jlo = jlo;
+  h->jhi = jhi;
+  // the staged kernel updates whole row blocks: slabs use the plain kernels
+  h->maps_ok = false;
+  h->tma_ty = h->tma_depth = 0;
+  return AHX_OK;
+}
+
+ahx_status ahx_row_bytes(ahx_handle* h, size_t* bytes) {
+  if (!h || !bytes) return fail(AHX_EINVAL, "live solver: null argument");
+  std::lock_guard<std::mutex> lk(h->mu);
+  if (ahx_status st = check(h)) return st;
+  const size_t per = (size_t)h->dims.nz * h->dims.nx;
+  *bytes = ((19 * per * h->esize + 15) & ~(size_t)15) + 7 * per * h->esize_g;   // f part padded to 16 bytes
+  return AHX_OK;
+}
+
+static ahx_status row_copy(ahx_handle* h, int j, void* buf, int to_buffer) {
+  if (!h || !buf) return fail(AHX_EINVAL, "live solver: null argument");
+  std::lock_guard<std::mutex> lk(h->mu);
+  if (ahx_status st = check(h)) return st;
+  if (j < 0 || j >= h->dims.ny) return fail(AHX_EINVAL, "live solver: row out of range");
+  AHX_CUDA(h, cudaSetDevice(h->dev));
+  const DomainView D = view(h);
+  AHX_CUDA(h, launch_row_copy(D, h->dims.precision, j, buf, to_buffer, h->s_step));
+  return AHX_OK;
+}
+
+ahx_status ahx_row_pack(ahx_handle* h, int j, void* dst_device) { return row_copy(h, j, dst_device, 1); }
+ahx_status ahx_row_unpack(ahx_handle* h, int j, const void* src_device) {
+  return row_copy(h, j, const_cast<void*>(src_device), 0);
 }
 
 ahx_status ahx_set_launch(ahx_handle* h, int block_y, int zslab) {

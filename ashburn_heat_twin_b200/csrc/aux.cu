@@ -219,6 +219,7 @@ __global__ void __launch_bounds__(256) stats_kernel(DomainView D, StatsScratch* 
     const int i = (int)(c % nx);
     const int j = (int)((c / nx) % ny);
     const int k = (int)(c / ((long)nx * ny));
+    if (j < D.jlo || j >= D.jhi) continue;   // ghost rows of a slab belong to its neighbour
     if (k < (int)__ldg(D.ktop + (long)j * nx + i)) continue;
     const uint32_t n = (uint32_t)k * D.ps + (uint32_t)j * (uint32_t)D.px + (uint32_t)i;
     R f[19];
@@ -300,6 +301,32 @@ __global__ void __launch_bounds__(256) export_plane_kernel(DomainView D, const T
   const R v = is_g ? K::dec_g(e) : K::dec_f(e, R(w));
   if (ref_is_f64) static_cast<double*>(ref)[c] = (double)v;
   else static_cast<float*>(ref)[c] = (float)v;
+}
+
+// one local row j of all 26 population planes <-> a packed buffer [f: 19][nz][nx], then (from the next 16-byte
+// boundary) [g: 7][nz][nx]; raw storage elements
+template <class TF, class TG>
+__global__ void __launch_bounds__(256) row_copy_kernel(DomainView D, int j, const void* f, const void* g, void* buf,
+                                                       int to_buffer) {
+  const long per = (long)D.nz * D.nx;
+  const long e = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= 26 * per) return;
+  const int q = (int)(e / per);
+  const int k = (int)((e % per) / D.nx), i = (int)(e % D.nx);
+  const uint32_t n = (uint32_t)k * D.ps + (uint32_t)j * (uint32_t)D.px + (uint32_t)i;
+  if (q < 19) {
+    TF* s = const_cast<TF*>(static_cast<const TF*>(f)) + (uint32_t)q * D.qs + n;
+    TF* b = static_cast<TF*>(buf) + (long)q * per + (long)k * D.nx + i;
+    if (to_buffer) *b = *s;
+    else *s = *b;
+  } else {
+    TG* s = const_cast<TG*>(static_cast<const TG*>(g)) + (uint32_t)(q - 19) * D.qs + n;
+    // the g part starts at the next 16-byte boundary after the f part
+    const size_t goff = (19 * (size_t)per * sizeof(TF) + 15) & ~(size_t)15;
+    TG* b = reinterpret_cast<TG*>(static_cast<unsigned char*>(buf) + goff) + (long)(q - 19) * per + (long)k * D.nx + i;
+    if (to_buffer) *b = *s;
+    else *s = *b;
+  }
 }
 
 template <class F>
@@ -392,6 +419,16 @@ cudaError_t launch_export_plane(const DomainView& D, int precision, const void* 
     else
       export_plane_kernel<StoreF<S>><<<grid, 256, 0, s>>>(D, static_cast<const StoreF<S>*>(src), ref_plane,
                                                           ref_is_f64, q, 0);
+    return cudaGetLastError();
+  });
+}
+
+cudaError_t launch_row_copy(const DomainView& D, int precision, int j, void* buf, int to_buffer, cudaStream_t s) {
+  return dispatch(precision, [&](auto tag) {
+    using S = decltype(tag);
+    const long total = 26L * D.nz * D.nx;
+    row_copy_kernel<StoreF<S>, StoreG<S>><<<(unsigned)((total + 255) / 256), 256, 0, s>>>(D, j, D.fA, D.gA, buf,
+                                                                                          to_buffer);
     return cudaGetLastError();
   });
 }

@@ -342,6 +342,7 @@ ahx_status check_members(const ahx_batch* b, ahx_handle* const* members, int cou
     if (ahx_status st = check(h)) return st;
     if (b && (h->dev != b->dev || h->dims.precision != b->precision || h->dims.arith != b->arith))
       return fail(AHX_EINVAL, "live solver: batch members must share device, precision and arithmetic");
+    if (h->nyg > 0) return fail(AHX_EINVAL, "live solver: a slab of a larger domain cannot join a batch");
   }
   return AHX_OK;
 }

@@ -111,18 +111,19 @@ __device__ __forceinline__ void load_column(const DomainView& D, const ParamsHea
 #pragma unroll
     for (int oy = 0; oy < 3; ++oy) km = max(km, C.kn[ox][oy]);
   C.kint = km + 1;
+  const int jg = j + D.jg0, nyg = D.nyg;   // global row: faces and sponges follow the whole domain
   C.latW = (i == 0);
   C.latE = (i == nx - 1);
-  C.latS = (j == 0);
-  C.latN = (j == ny - 1);
+  C.latS = (jg == 0);
+  C.latN = (jg == nyg - 1);
   C.face = C.latW || C.latE || C.latS || C.latN;
   C.onb = (C.latW && P.inflow_w == 0) || (C.latE && P.inflow_e == 0) || (C.latS && P.inflow_s == 0) ||
           (C.latN && P.inflow_n == 0);
   int dmin = 1000;
   if (P.inflow_w == 0 && i < dmin) dmin = i;
   if (P.inflow_e == 0 && nx - 1 - i < dmin) dmin = nx - 1 - i;
-  if (P.inflow_s == 0 && j < dmin) dmin = j;
-  if (P.inflow_n == 0 && ny - 1 - j < dmin) dmin = ny - 1 - j;
+  if (P.inflow_s == 0 && jg < dmin) dmin = jg;
+  if (P.inflow_n == 0 && nyg - 1 - jg < dmin) dmin = nyg - 1 - jg;
   C.spon = dmin < P.nsw;
   C.spg = R(0);
   if (C.spon) {
@@ -635,7 +636,7 @@ __device__ __forceinline__ void step_block(const DomainView& D, int bx, int by, 
   // A warp is one row of 32 columns. It walks the levels in lockstep from its lowest first fluid level, so the lanes
   // of one load touch one level (coalesced), and it takes the interior fast path only when every active lane is
   // interior (the general path gives identical values for interior cells, so a mixed level runs one path, not two).
-  const bool valid = i < D.nx && j < D.ny;
+  const bool valid = i < D.nx && j >= D.jlo && j < D.jhi;
   Column<R> C;
   int kstart = k1;
   if (valid) {

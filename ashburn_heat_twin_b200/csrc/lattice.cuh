@@ -191,6 +191,9 @@ struct DomainView {
   double* facc;
   int* err;                     // error word: a staged copy that did not arrive in time sets it
   int nx, ny, nz, px;
+  // y-slab of a larger domain: local row 0 is global row jg0 of nyg; only local rows [jlo, jhi) are updated (the
+  // others are ghost rows refreshed from the neighbouring slabs); a whole domain has jg0 0, nyg ny, [0, ny)
+  int jg0, nyg, jlo, jhi;
   uint32_t ps;                  // plane stride px*ny
   uint32_t qs;                  // q stride px*ny*nz
   // element offset of the interior pull source of population q relative to the cell: q*qs - (cx + cy*px + cz*ps)

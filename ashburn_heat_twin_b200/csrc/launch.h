@@ -78,6 +78,9 @@ cudaError_t launch_import_plane(const DomainView& D, int precision, const void* 
 cudaError_t launch_export_plane(const DomainView& D, int precision, const void* src, void* ref_plane, int ref_is_f64,
                                 int q, int is_g, cudaStream_t s);
 
+// copy local row j of all 26 planes of the current state (D.fA / D.gA) to (to_buffer) or from a packed device buffer
+cudaError_t launch_row_copy(const DomainView& D, int precision, int j, void* buf, int to_buffer, cudaStream_t s);
+
 int element_bytes(int precision);     // bytes of one stored flow population f
 int element_bytes_g(int precision);   // bytes of one stored temperature population g
 

@@ -26,7 +26,8 @@ SYMBOLS = ('ahx_create', 'ahx_destroy', 'ahx_last_error', 'ahx_get_info', 'ahx_s
            'ahx_read_state_f64', 'ahx_write_state_f64', 'ahx_read_dbg', 'ahx_clear_dbg', 'ahx_stats',
            'ahx_budget_enable', 'ahx_budget_read', 'ahx_set_launch', 'ahx_autotune', 'ahx_time_steps', 'ahx_stats_noalloc',
            'ahx_batch_create', 'ahx_batch_step', 'ahx_batch_time_steps', 'ahx_batch_sync', 'ahx_batch_set_launch',
-           'ahx_batch_get_info', 'ahx_batch_destroy', 'ahx_batch_set_members', 'ahx_accum_enable', 'ahx_accum_read')
+           'ahx_batch_get_info', 'ahx_batch_destroy', 'ahx_batch_set_members', 'ahx_accum_enable', 'ahx_accum_read',
+           'ahx_set_slab', 'ahx_row_bytes', 'ahx_row_pack', 'ahx_row_unpack')
 
 
 class AhxError(RuntimeError):
@@ -115,6 +116,10 @@ def load_library(path: str = LIB_PATH):
         'ahx_batch_set_launch': [H, i, i, i, i],
         'ahx_batch_set_members': [H, ctypes.POINTER(H), i],
         'ahx_accum_enable': [H, i],
+        'ahx_set_slab': [H, i, i, i, i],
+        'ahx_row_bytes': [H, ctypes.POINTER(ctypes.c_size_t)],
+        'ahx_row_pack': [H, i, vp],
+        'ahx_row_unpack': [H, i, vp],
         'ahx_accum_read': [H, vp, vp, ctypes.POINTER(ctypes.c_int64), i],
         'ahx_batch_get_info': [H, ctypes.POINTER(BatchInfoOut)],
         'ahx_batch_destroy': [H],
@@ -335,6 +340,21 @@ class CudaDevice:
 
     def set_launch(self, block_y=0, zslab=0):
         self._c('ahx_set_launch', int(block_y), int(zslab))
+
+    def set_slab(self, jg0, nyg, jlo, jhi):
+        self._c('ahx_set_slab', int(jg0), int(nyg), int(jlo), int(jhi))
+
+    def row_bytes(self):
+        b = ctypes.c_size_t()
+        self._c('ahx_row_bytes', ctypes.byref(b))
+        return b.value
+
+    def row_pack(self, j, dst_ptr):
+        """queue a copy of local row j (26 planes) of the current state into device memory at dst_ptr"""
+        self._c('ahx_row_pack', int(j), ctypes.c_void_p(int(dst_ptr)))
+
+    def row_unpack(self, j, src_ptr):
+        self._c('ahx_row_unpack', int(j), ctypes.c_void_p(int(src_ptr)))
 
     def accum_enable(self, on=True):
         self._c('ahx_accum_enable', int(bool(on)))

@@ -1,0 +1,137 @@
+"""One domain split into y-slabs (rows), one libahx handle per slab: the single-domain decomposition for grids beyond
+one GPU's share (a 5 m grid, 1200x1200x128, needs ~100 GB in FP32).
+
+The host builds the whole domain once (the live solver's own domain and parameter code, on a recording device that
+only keeps the host images) and gives each slab its rows of the column records and the ktop plane, plus one ghost row
+on each internal boundary. Every step is: each slab steps its own rows (faces and sponges follow the global rows);
+then each slab's boundary rows are packed into device buffers and unpacked into the neighbours' ghost rows. On one
+device the copies stay on the device; across GPUs the packed rows go over NCCL (send / recv of 26 x nz x nx
+elements per boundary per step) with one process per slab. The stepped rows are bit-identical to the undivided
+domain's.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import solver as S
+
+
+class _Recorder:
+    """A device that keeps the host images the live solver uploads and does nothing else."""
+
+    def __init__(self, nx, ny, nz):
+        self.nx, self.ny, self.nz = nx, ny, nz
+        self.params = self.colv = self.ktop = None
+        self._p = 0
+        self.adapter = 'host images'
+
+    def set_params(self, b):
+        self.params = bytes(b)
+
+    def set_columns(self, colv):
+        self.colv = np.array(colv, np.uint32).reshape(self.ny, self.nx, 4)
+
+    def set_ktop(self, ktop, oldk):
+        self.ktop = np.array(ktop, np.uint32).reshape(self.ny, self.nx)
+
+    def set_parity(self, p):
+        self._p = int(p)
+
+    def parity(self):
+        return self._p
+
+    def init_flow(self):
+        pass
+
+    def clear_heat(self):
+        pass
+
+    def sync(self, timeout_s=None):
+        pass
+
+    def lost(self):
+        return None
+
+    def destroy(self):
+        pass
+
+
+def slab_rows(ny, nslabs):
+    """Owned global rows [a, b) of each slab, as even as possible."""
+    edges = np.linspace(0, ny, nslabs + 1).round().astype(int)
+    return [(int(edges[r]), int(edges[r + 1])) for r in range(nslabs)]
+
+
+class SlabDomain:
+    """The domain of create_live_solver(**opts) split into `nslabs` y-slabs on one device (`device`), each a CudaDevice
+    with precision / arithmetic as given. step(n) advances every slab n steps with a ghost-row exchange after each."""
+
+    def __init__(self, nslabs, precision='fp32', arith='exact', device=None, **opts):
+        from .cuda_device import CudaDevice
+        rec = {}
+
+        def recorder(nx, ny, nz):
+            rec['dev'] = _Recorder(nx, ny, nz)
+            return rec['dev']
+
+        self.host = S.create_live_solver(backend=recorder, **opts)
+        img = rec['dev']
+        self.nx, self.ny, self.nz = img.nx, img.ny, img.nz
+        self.rows = slab_rows(self.ny, nslabs)
+        self.slabs = []
+        for a, b in self.rows:
+            ga, gb = int(a > 0), int(b < self.ny)
+            jg0, nyl = a - ga, (b - a) + ga + gb
+            d = CudaDevice(self.nx, nyl, self.nz, device=device, precision=precision, arith=arith)
+            d.set_slab(jg0, self.ny, ga, ga + (b - a))
+            d.set_params(img.params)
+            d.set_columns(np.ascontiguousarray(img.colv[jg0:jg0 + nyl]).reshape(-1, 4))
+            d.set_ktop(np.ascontiguousarray(img.ktop[jg0:jg0 + nyl]).reshape(-1), None)
+            d.init_flow()
+            d.clear_heat()
+            self.slabs.append(dict(dev=d, a=a, b=b, jg0=jg0, ny=nyl, lo=ga, hi=ga + (b - a)))
+        import torch
+        nb = (self.slabs[0]['dev'].row_bytes() + 255) // 256 * 256   # keep the second half 256-byte aligned
+        self._buf = [torch.empty(2 * nb, dtype=torch.uint8, device=f'cuda:{device or 0}')
+                     for _ in range(len(self.slabs) - 1)]
+        self._nb = nb
+        self.steps = 0
+
+    def exchange(self):
+        """refresh every ghost row from the neighbouring slab's boundary row (device copies, in order)"""
+        for r in range(len(self.slabs) - 1):
+            lo, hi = self.slabs[r], self.slabs[r + 1]
+            buf = self._buf[r]
+            p0, p1 = buf.data_ptr(), buf.data_ptr() + self._nb
+            lo['dev'].row_pack(lo['hi'] - 1, p0)        # south slab's last owned row -> north slab's ghost row 0
+            hi['dev'].row_pack(hi['lo'], p1)            # north slab's first owned row -> south slab's top ghost row
+            lo['dev'].sync()
+            hi['dev'].sync()
+            hi['dev'].row_unpack(0, p0)
+            lo['dev'].row_unpack(lo['ny'] - 1, p1)
+        for s in self.slabs:
+            s['dev'].sync()
+
+    def step(self, n=1):
+        for _ in range(int(n)):
+            for s in self.slabs:
+                s['dev'].step(1, 0)
+            self.exchange()
+            self.steps += 1
+
+    def read_state(self):
+        """f (19, nz, ny, nx) and g (7, nz, ny, nx) of the whole domain, from the slabs' owned rows."""
+        f = np.empty((19, self.nz, self.ny, self.nx), np.float32)
+        g = np.empty((7, self.nz, self.ny, self.nx), np.float32)
+        for s in self.slabs:
+            fl, gl = s['dev'].read_state()
+            fl = fl.reshape(19, self.nz, s['ny'], self.nx)
+            gl = gl.reshape(7, self.nz, s['ny'], self.nx)
+            f[:, :, s['a']:s['b']] = fl[:, :, s['lo']:s['hi']]
+            g[:, :, s['a']:s['b']] = gl[:, :, s['lo']:s['hi']]
+        return f, g
+
+    def destroy(self):
+        for s in self.slabs:
+            s['dev'].destroy()
+        self.slabs = []

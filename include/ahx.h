@@ -223,6 +223,21 @@ ahx_status ahx_autotune(ahx_handle* h, int steps_per_trial, int* best_block_y, i
 ahx_status ahx_stats_noalloc(int nx, int ny, int nz, const float* f, const float* g, const uint32_t* ktop,
                              ahx_stats_out* out, void* stream);
 
+/* --- y-slab decomposition of one domain ----------------------------------------------------------------------- */
+
+/* No counterpart in the reference (one domain per device). A handle can hold rows [jg0, jg0 + ny) of a domain nyg
+ * rows tall and update only its local rows [jlo, jhi); the other local rows are ghost copies of the neighbouring
+ * slabs' boundary rows, refreshed after every step by copying packed rows between slabs (ahx_row_pack on one,
+ * ahx_row_unpack on the other; device buffers, ordered on each handle's stream; over NCCL between GPUs). Lateral
+ * faces and the outflow sponge follow the global rows, so the stepped rows are bit-identical to the undivided
+ * domain's. Slabs use the plain kernels (no staged kernel, no batches); stats count only the updated rows. */
+ahx_status ahx_set_slab(ahx_handle* h, int jg0, int nyg, int jlo, int jhi);
+/* bytes of a packed row: [19][nz][nx] f elements, padded to 16 bytes, then [7][nz][nx] g elements; the buffers given
+ * to ahx_row_pack / ahx_row_unpack must be 16-byte aligned */
+ahx_status ahx_row_bytes(ahx_handle* h, size_t* bytes);
+ahx_status ahx_row_pack(ahx_handle* h, int j, void* dst_device);
+ahx_status ahx_row_unpack(ahx_handle* h, int j, const void* src_device);
+
 /* --- batched stepping ----------------------------------------------------------------------------------------- */
 
 /* No counterpart in the reference, which steps one domain per device (solver.js:401-427). A batch groups handles of
