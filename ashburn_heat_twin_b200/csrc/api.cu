@@ -941,7 +941,7 @@ ahx_status ahx_autotune(ahx_handle* h, int steps_per_trial, int* best_block_y, i
     for (Shape sh : {Shape{4, 0, 4, 2, false}, Shape{4, 0, 4, 3, false}, Shape{4, 0, 4, 4, false},
                      Shape{8, 0, 8, 2, false}, Shape{8, 0, 8, 3, false}})
       shapes.push_back(sh);
-  std::vector<int> zss = {h->dims.nz, 32, 16, 8};
+  std::vector<int> zss = {h->dims.nz, 32, 16, 12, 8, 6};
   float best = 1e30f;
   int bby = h->block_y, bzs = h->zslab, bmb = h->minb, bty = h->tma_ty, bdp = h->tma_depth;
   bool bpr = h->pairs;
