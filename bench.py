@@ -333,11 +333,17 @@ def main_serve(a, rank, world, local, dist, torch):
     warm = SV.requests_from_trace(SC.serve_trace(st, 6, 1000.0, seed=a.seed + 100), sim_s=5.0)
     srv.run(warm, timeout_s=300)
     srv.cell_updates = srv.launch_chunks = srv.rebuilds = srv.evictions = srv.batch_steps = 0
-    reqs = SV.requests_from_trace(SC.serve_trace(st, a.requests, a.rate, seed=a.seed), sim_s=SC.SERVE_SIM_S)
+    # each rank serves its own trace (replicas: seed + rank); the job's rate is all ranks' cell updates over the
+    # longest makespan
+    reqs = SV.requests_from_trace(SC.serve_trace(st, a.requests, a.rate, seed=a.seed + rank), sim_s=SC.SERVE_SIM_S)
+    if dist is not None:
+        dist.barrier()
     srv.chunk_log = []
     with Clocks(local) as clk:
         stats = srv.run(reqs, timeout_s=900)
     clocks = clk.summary()
+    makespan_all = RP.max_over_ranks(stats['makespan_s'], dist, f'cuda:{local}')
+    job_glups = RP.aggregate_rate(stats['cell_updates'], world, makespan_all) / 1e9
     # device-busy estimate from the chunk completions the host observed (queue depth keeps the device fed)
     busy, last = 0.0, 0.0
     for issued, k, cells_, members, fin in srv.chunk_log:
@@ -366,7 +372,7 @@ def main_serve(a, rank, world, local, dist, torch):
     classes = {f'{int(k[0])} m': dict(solo_glups=v / 1e9) for k, v in rate.items()}
     srv.close()
     out = dict(metric='GLUPS (all cells) served with continuous batching, Poisson trace of live-solver requests',
-               value=stats['glups'], unit='GLUPS', n_gpus=world, steps=stats['batch_steps'], warmup=6,
+               value=job_glups, unit='GLUPS', n_gpus=world, steps=stats['batch_steps'], warmup=6,
                ms_per_step=stats['makespan_s'] * 1e3 / max(1, stats['batch_steps']), higher_is_better=True,
                scaling='weak', vs_baseline=None,
                dtype=DTYPE[a.precision],
@@ -386,11 +392,14 @@ def main_serve(a, rank, world, local, dist, torch):
                            what='the same trace solved back to back in arrival order, each request alone at its '
                                 'class solo device rate (host work not counted)'),
                roofline=None, cpu_baseline=None,
-               e2e=dict(value=stats['glups'], unit='GLUPS', h2d_bytes_per_step=h2d / steps_total,
+               e2e=dict(value=job_glups, unit='GLUPS', h2d_bytes_per_step=h2d / steps_total,
                         d2h_bytes_per_step=d2h / steps_total,
                         what='the served rate is end to end: request set-up uploads, batched steps and read() '
                              'downloads are all inside the wall-clock makespan'),
                gpu_launches=stats['batch_steps'], clocks=clocks)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(out), flush=True)
     return 0
@@ -494,6 +503,9 @@ def main_precision(a, rank, world, local, dist, torch):
                            near_ground='first fluid cell of each column, mean over the window',
                            parallelism=f'replicas x{world}'),
                precision=prec, roofline=None, cpu_baseline=None, e2e=None, gpu_launches=a.steps)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(out), flush=True)
     return 0
