@@ -37,6 +37,17 @@ WORKLOADS = {
                     '211 DC roofs', dx=10, heightM=640, met='C2_MET', spec='C2'),
     'c1': dict(desc='200x200x32 cells at 30 m (1.28 M), synthetic seed 1: 8 hills 0-30 m, 1500 buildings, '
                     '60 DC roofs', dx=30, heightM=960, met='C1_MET', spec='C1'),
+    # the reference's own Ashburn planes (tests/golden/static10.*) at the grids its published step rates use
+    # (js/live/README.md:226-238): 20 m 300x300x36, 30 m 200x200x24, 40 m 150x150x18; met of its validation page
+    'r20': dict(desc='the Ashburn 6 km box at 20 m (300x300x36, 3.24 M cells), reference planes, validation met',
+                dx=20, heightM=720, real=True, published_glups=4.28,
+                published='RTX 4090 WebGPU 4,280 MLUPS, read() 4.2 / 9.9 ms median / max (js/live/README.md:232)'),
+    'r30': dict(desc='the Ashburn 6 km box at 30 m (200x200x24, 0.96 M cells), reference planes, validation met',
+                dx=30, heightM=720, real=True, published_glups=4.10,
+                published='RTX 4090 WebGPU 4,100 MLUPS, read() 3.2 / 4.7 ms median / max (js/live/README.md:233)'),
+    'r40': dict(desc='the Ashburn 6 km box at 40 m (150x150x18, 0.405 M cells), reference planes, validation met',
+                dx=40, heightM=720, real=True, published_glups=6.60,
+                published='RTX 4090 WebGPU 6,600 MLUPS, read() 3.0 / 5.3 ms median / max (js/live/README.md:234)'),
     'c2q': dict(desc='300x300x64 cells at 10 m (5.76 M), synthetic seed 3: 6 hills 0-40 m, 1000 buildings, '
                      '53 DC roofs', dx=10, heightM=640, met='C2_MET', spec='C2Q'),
     'c3': dict(desc='precision study on 600x600x64 at 10 m (config c2): FP32 / FP16 / BF16 storage against the FP64 '
@@ -64,9 +75,14 @@ def make_solver(backend=None, device=None, precision='fp32', arith='exact', work
     from ashburn_heat_twin_b200 import solver as S
     from ashburn_heat_twin_b200 import synth
     w = WORKLOADS[workload]
-    st = synth.make_static10(getattr(synth, w['spec']))
-    kw = dict(static=st, dx=w['dx'], allowAnyDx=True, heightM=w['heightM'], u10Max=8, alpha=0.2,
-              met=getattr(synth, w['met']), existingFlux=400)
+    if w.get('real'):
+        # the reference's validation settings (tests/live/validate.html:29,61-75): u10Max 8, alpha 0.14, flux 400
+        kw = dict(base=os.path.join(ROOT, 'tests', 'golden'), dx=w['dx'], heightM=w['heightM'], u10Max=8,
+                  met=dict(u10=3.09, dirFrom=210, wstar=1.67, blh=903, ustar=0.32), existingFlux=400)
+    else:
+        st = synth.make_static10(getattr(synth, w['spec']))
+        kw = dict(static=st, dx=w['dx'], allowAnyDx=True, heightM=w['heightM'], u10Max=8, alpha=0.2,
+                  met=getattr(synth, w['met']), existingFlux=400)
     if backend is None:
         from ashburn_heat_twin_b200.cuda_device import CudaDevice
 
@@ -140,11 +156,11 @@ class Clocks:
                     if any(r[3].strip().replace('.', '', 1).isdigit() for r in rows) else None)
 
 
-def cpu_baseline(seconds=10.0, max_steps=30):
-    """The oracle (CPU restatement of the reference kernels) on full 600x600x64 steps, all host threads."""
+def cpu_baseline(seconds=10.0, max_steps=30, workload='c2'):
+    """The oracle (CPU restatement of the reference kernels) on full steps of the workload, all host threads."""
     import numpy as np
     from oracle import oracle as O
-    s = make_solver(backend=lambda nx, ny, nz: O.OracleDevice(nx, ny, nz))
+    s = make_solver(backend=lambda nx, ny, nz: O.OracleDevice(nx, ny, nz), workload=workload)
     threads = O.max_threads()
     dev = s._dev
     t0 = time.perf_counter()
@@ -157,7 +173,8 @@ def cpu_baseline(seconds=10.0, max_steps=30):
     cells = s.info['nCells']
     s.destroy()
     return dict(value=cells * n / t / 1e9, unit='GLUPS', cores=threads, kind='port',
-                sample=f'{n} full steps of the 600x600x64 domain ({cells * n / 1e6:.0f} M cell updates, {t:.1f} s)')
+                sample=f'{n} full steps of the {s.info["nx"]}x{s.info["ny"]}x{s.info["nz"]} domain '
+                       f'({cells * n / 1e6:.0f} M cell updates, {t:.1f} s)')
 
 
 def run_reference(a, rank):
@@ -525,8 +542,9 @@ def main():
     ap.add_argument('--block-y', type=int, default=0, help='fix the launch shape instead of autotuning')
     ap.add_argument('--zslab', type=int, default=0)
     ap.add_argument('--workload', default='c2', choices=sorted(WORKLOADS),
-                    help='c2 (the benchmark), c1 / c2q (smaller cases for profiling), c3 (storage precision study), '
-                         'c4 (64 domains in one batch), c5 (serving)')
+                    help='c2 (the benchmark), c1 / c2q (smaller cases for profiling), r20 / r30 / r40 (the reference\'s '
+                         'Ashburn planes at its published grids), c3 (storage precision study), c4 (64 domains in one '
+                         'batch), c5 (serving)')
     ap.add_argument('--members', type=int, default=64, help='batch: scenarios in the batch (64 = the full set)')
     ap.add_argument('--requests', type=int, default=48, help='serving: requests in the trace')
     ap.add_argument('--rate', type=float, default=50.0, help='serving: mean arrival rate (requests/s)')
@@ -599,7 +617,10 @@ def main():
     from ashburn_heat_twin_b200 import synth
     F = a.frame
     frames = max(10, 2 * a.steps)        # long enough that pipeline fill and drain stay a few per cent
-    met = dict(synth.C2_MET)
+    wl = WORKLOADS[a.workload]
+    met = dict(u10=3.09, dirFrom=210, wstar=1.67, blh=903, ustar=0.32) if wl.get('real') else \
+        dict(getattr(synth, wl['met']))
+    u10_0 = met['u10']
     pend = []
     s.setMet(met)
     s.step(F)
@@ -607,7 +628,7 @@ def main():
     barrier()
     t0 = time.perf_counter()
     for fr in range(frames):
-        met['u10'] = 3.5 + 0.01 * (fr % 5)          # a new parameter block every frame (host -> device)
+        met['u10'] = u10_0 + 0.01 * (fr % 5)        # a new parameter block every frame (host -> device)
         s.setMet(met)
         s.step(F)
         pend.append(s.read(vol=True, wind=True))
@@ -623,20 +644,33 @@ def main():
     e2e = dict(value=world * cells * F * frames / e2e_s / 1e9, unit='GLUPS', h2d_bytes_per_step=h2d / F,
                d2h_bytes_per_step=d2h / F, frame_steps=F, frames=frames,
                per_frame='setMet (parameter block H2D) + step(F) + read(vol, wind) D2H')
+    # read() latency on an idle device (the reference publishes its median / max, js/live/README.md:232-234)
+    lat = []
+    for _ in range(20):
+        s.step(F).result()
+        t1 = time.perf_counter()
+        s.read(vol=True, wind=True).result()
+        lat.append((time.perf_counter() - t1) * 1e3)
+    lat.sort()
+    read_ms = dict(median=lat[len(lat) // 2], max=lat[-1], reads=len(lat),
+                   what='read(vol, wind) after the steps finished: surface and volume kernels, D2H, host arrays')
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         s_steps = s._steps
-        cpu = cpu_baseline()
+        cpu = cpu_baseline(workload=a.workload)
         del s_steps
-    metric = METRIC.replace('600x600x64', WORKLOADS[a.workload]['desc'].split(' cells')[0])
+    metric = METRIC.replace('600x600x64', f'{nx}x{ny}x{nz}')
+    vs = value / wl['published_glups'] if wl.get('published_glups') else None
     out = dict(metric=metric, value=value, unit='GLUPS', n_gpus=world, steps=a.steps, warmup=a.warmup,
-               ms_per_step=ms_all / a.steps, higher_is_better=True, scaling='weak', vs_baseline=None,
+               ms_per_step=ms_all / a.steps, higher_is_better=True, scaling='weak', vs_baseline=vs,
                dtype=DTYPE[a.precision],
-               data='synthetic (seeded terrain and buildings; no public dataset involved)',
+               data=('the reference\'s own Ashburn planes (tests/golden/static10.*)' if wl.get('real') else
+                     'synthetic (seeded terrain and buildings; no public dataset involved)'),
                config=dict(workload=WORKLOADS[a.workload]['desc'], precision=a.precision, arith=a.arith, scheme='pull',
                            parallelism=f'replicas x{world}', fluid_cells=fluid, l2=f"state {s._dev.info()['state_bytes'] / 1e9:.2f} GB vs 126 MB L2",
-                           launch=dict(block_y=tune[0], zslab=tune[1]) if tune else None),
-               roofline=roof, cpu_baseline=cpu, e2e=e2e, gpu_launches=a.steps, clocks=clocks,
+                           launch=dict(block_y=tune[0], zslab=tune[1]) if tune else None,
+                           published=wl.get('published')),
+               roofline=roof, cpu_baseline=cpu, e2e=e2e, read_ms=read_ms, gpu_launches=a.steps, clocks=clocks,
                glups_fluid=world * fluid * a.steps / (ms_all / 1e3) / 1e9)
     s.destroy()
     if dist is not None:
