@@ -187,6 +187,8 @@ void free_all(ahx_handle* h) {
   cudaSetDevice(h->dev);
   if (h->s_step) cudaStreamSynchronize(h->s_step);
   if (h->s_copy) cudaStreamSynchronize(h->s_copy);
+  for (auto& g : h->graph)
+    if (g) cudaGraphExecDestroy(g), g = nullptr;
   for (int p = 0; p < 2; ++p) {
     if (h->f[p]) cudaFree(h->f[p]);
     if (h->g[p]) cudaFree(h->g[p]);
@@ -441,6 +443,53 @@ ahx_status ahx_set_parity(ahx_handle* h, int parity) {
   return AHX_OK;
 }
 
+// Everything a plain step's launches depend on besides the parity (buffers and tables are fixed per handle).
+uint64_t launch_key(const ahx_handle* h, const StepLaunch& L) {
+  uint64_t k = 1469598103934665603ull;
+  const int v[] = {L.precision, L.block_y, L.zslab, L.minb, (int)L.pairs, L.tma_ty, L.tma_depth,
+                   h->jg0, h->nyg, h->jlo, h->jhi, h->dims.arith};
+  for (int x : v) k = (k ^ (uint64_t)(uint32_t)x) * 1099511628211ull;
+  return k | 1;   // never 0, the "no graph" key
+}
+
+// two plain steps starting at parity p, captured once per launch set-up and replayed (launch gaps matter for small
+// grids, where a step takes tens of microseconds)
+ahx_status step_graph(ahx_handle* h, const StepLaunch& L0, int p, cudaGraphExec_t* out) {
+  const uint64_t key = launch_key(h, L0);
+  if (h->graph[p] && h->graph_key[p] == key) {
+    *out = h->graph[p];
+    return AHX_OK;
+  }
+  if (h->graph[p]) cudaGraphExecDestroy(h->graph[p]);
+  h->graph[p] = nullptr;
+  h->graph_key[p] = 0;
+  cudaGraph_t g = nullptr;
+  AHX_CUDA(h, cudaStreamBeginCapture(h->s_step, cudaStreamCaptureModeThreadLocal));
+  cudaError_t e = cudaSuccess;
+  for (int s = 0; s < 2 && e == cudaSuccess; ++s) {
+    StepLaunch L = L0;
+    L.mode = 0;
+    const int par = p ^ s;
+    L.maps = L.tma_ty ? &h->maps[L.tma_ty == 8 ? 1 : 0][par] : nullptr;
+    const DomainView D = view_at(h, par);
+    e = h->dims.arith == AHX_ARITH_FAST ? fast::launch_step(D, L, h->s_step) : exact::launch_step(D, L, h->s_step);
+  }
+  const cudaError_t e2 = cudaStreamEndCapture(h->s_step, &g);
+  if (e != cudaSuccess || e2 != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    return cuda_fail(h, e != cudaSuccess ? e : e2, "step graph capture");
+  }
+  const cudaError_t e3 = cudaGraphInstantiate(&h->graph[p], g, 0);
+  cudaGraphDestroy(g);
+  if (e3 != cudaSuccess) {
+    h->graph[p] = nullptr;
+    return cuda_fail(h, e3, "step graph instantiate");
+  }
+  h->graph_key[p] = key;
+  *out = h->graph[p];
+  return AHX_OK;
+}
+
 ahx_status ahx_step(ahx_handle* h, int n, int mode) {
   if (!h) return fail(AHX_EINVAL, "live solver: null handle");
   std::lock_guard<std::mutex> lk(h->mu);
@@ -458,7 +507,17 @@ ahx_status ahx_step(ahx_handle* h, int n, int mode) {
   L.pairs = h->pairs;
   L.tma_ty = h->maps_ok ? h->tma_ty : 0;
   L.tma_depth = h->tma_depth;
-  for (int s = 0; s < n; ++s) {
+  int s = 0;
+  if (mode == AHX_MODE_NONE && !L.budget && n >= 2) {
+    // pairs of plain steps from the captured graph of the current parity
+    cudaGraphExec_t g = nullptr;
+    if (ahx_status st = step_graph(h, L, h->parity, &g)) return st;
+    for (; s + 2 <= n; s += 2) {
+      AHX_CUDA(h, cudaGraphLaunch(g, h->s_step));
+      h->steps += 2;
+    }
+  }
+  for (; s < n; ++s) {
     L.mode = (mode == AHX_MODE_ACC) ? 2 : ((mode == AHX_MODE_OUT && s == n - 1) ? 1 : 0);
     L.maps = L.tma_ty ? &h->maps[L.tma_ty == 8 ? 1 : 0][h->parity] : nullptr;
     DomainView D = view(h);

@@ -74,6 +74,8 @@ struct ahx_handle {
   int block_y = 4, zslab = 0, minb = 0;
   bool pairs = false;                     // paired levels on packed f32x2 arithmetic (FMA build)
   int jg0 = 0, nyg = 0, jlo = 0, jhi = 0;   // y-slab of a larger domain (nyg = 0: the whole domain)
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};   // two plain steps starting at parity 0 / 1
+  uint64_t graph_key[2] = {0, 0};                 // launch set-up each graph was captured with
   int tma_ty = 0, tma_depth = 0;          // staged kernel selected when tma_ty > 0
   bool maps_ok = false;
   ahx::TmaMaps maps[2][2];                     // [TY 4 / 8][parity]: tensor maps of the state read by a step
