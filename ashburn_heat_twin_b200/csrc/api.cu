@@ -74,6 +74,8 @@ DomainView ahx::view_at(ahx_handle* h, int parity) {
   D.sacc = h->accum_on ? h->d_sacc : nullptr;
   D.facc = h->accum_on ? h->d_facc : nullptr;
   D.err = h->d_err;
+  D.tick = h->d_tick;
+  D.tick_blocks = 0;
   D.nx = h->dims.nx;
   D.ny = h->dims.ny;
   D.nz = h->dims.nz;
@@ -195,7 +197,7 @@ void free_all(ahx_handle* h) {
     h->f[p] = h->g[p] = nullptr;
   }
   void* devs[] = {h->d_params, h->d_colv, h->d_ktop, h->d_oldk, h->d_dbg, h->d_budget, h->d_stats, h->d_err,
-                  h->d_sacc, h->d_facc};
+                  h->d_tick, h->d_sacc, h->d_facc};
   for (void* p : devs)
     if (p) cudaFree(p);
   h->d_params = nullptr;
@@ -206,6 +208,7 @@ void free_all(ahx_handle* h) {
   h->d_sacc = h->d_facc = nullptr;
   h->d_stats = nullptr;
   h->d_err = nullptr;
+  h->d_tick = nullptr;
   for (auto& r : h->reads) {
     if (r.d_surf) cudaFree(r.d_surf);
     if (r.d_vol) cudaFree(r.d_vol);
@@ -314,10 +317,12 @@ ahx_status ahx_create(const ahx_dims* dims, ahx_handle** out) {
       cudaMalloc(&h->d_ktop, NXY * 4) != cudaSuccess || cudaMalloc(&h->d_oldk, NXY * 4) != cudaSuccess ||
       cudaMalloc(&h->d_budget, (size_t)kBudgetSlots * kBudgetStride * sizeof(double)) != cudaSuccess ||
       cudaMalloc(&h->d_stats, sizeof(StatsScratch)) != cudaSuccess ||
-      cudaMalloc(&h->d_err, sizeof(int)) != cudaSuccess)
+      cudaMalloc(&h->d_err, sizeof(int)) != cudaSuccess || cudaMalloc(&h->d_tick, 4 * sizeof(uint32_t)) != cudaSuccess)
     return bail(AHX_ENOMEM, "live solver: buffer allocation failed (out of memory)");
   cudaMemsetAsync(h->d_err, 0, sizeof(int), h->s_step);
-  h->maps_ok = h->esize == h->esize_g;   // the staged kernel stages f and g with one element size
+  cudaMemsetAsync(h->d_tick, 0, 4 * sizeof(uint32_t), h->s_step);
+  // the staged kernel stages f and g with one element size and rounds to nearest
+  h->maps_ok = h->esize == h->esize_g && dims->precision != AHX_FP16_SR;
   for (int t = 0; t < 2 && h->maps_ok; ++t)
     for (int p = 0; p < 2; ++p) h->maps_ok = h->maps_ok && make_maps(h, h->f[p], h->g[p], t ? 8 : 4, &h->maps[t][p]);
   cudaMemsetAsync(h->d_params, 0, 64 + 16 * (size_t)dims->nz, h->s_step);
@@ -1000,12 +1005,14 @@ ahx_status ahx_autotune(ahx_handle* h, int steps_per_trial, int* best_block_y, i
     for (Shape sh : {Shape{4, 0, 4, 2, false}, Shape{4, 0, 4, 3, false}, Shape{4, 0, 4, 4, false},
                      Shape{8, 0, 8, 2, false}, Shape{8, 0, 8, 3, false}})
       shapes.push_back(sh);
-  std::vector<int> zss = {h->dims.nz, 32, 16, 12, 8, 6};
+  // thin slabs put more blocks in flight on small grids, where one 6-level wave leaves the SMs latency-bound
+  std::vector<int> zss = {h->dims.nz, 32, 16, 12, 8, 6, 4, 3, 2};
   float best = 1e30f;
   int bby = h->block_y, bzs = h->zslab, bmb = h->minb, bty = h->tma_ty, bdp = h->tma_depth;
   bool bpr = h->pairs;
   DomainView D = view(h);
   D.dbg = nullptr;
+  D.tick = h->d_tick + 2;   // trials advance a scratch step counter, not the handle's
   StepLaunch L;
   L.precision = h->dims.precision;
   L.mode = 0;

@@ -15,6 +15,7 @@ int element_bytes(int precision) {
     case 3: return 8;
     case 4: return 2;   // f FP16, g f32
     case 5: return 2;   // f BF16, g f32
+    case 6: return 2;   // FP16, stochastic rounding in the step
     default: return 0;
   }
 }
@@ -338,6 +339,7 @@ cudaError_t dispatch(int precision, F&& f) {
     case 3: return f(double{});
     case 4: return f(Mixed<__half, float>{});
     case 5: return f(Mixed<__nv_bfloat16, float>{});
+    case 6: return f(half_sr{});
     default: return cudaErrorInvalidValue;
   }
 }

@@ -245,6 +245,10 @@ ahx_status upload(ahx_batch* b, const std::vector<ahx_handle*>& mem, const std::
     ahx_handle* h = mem[m];
     g.views[m] = view_at(h, h->parity);
     g.views[C + m] = view_at(h, h->parity ^ 1);
+    // tiles of this member in one step (its blocks report done to its step counter)
+    const uint32_t nt = (uint32_t)((h->dims.nx + 31) / 32) * (uint32_t)((h->dims.ny + 3) / 4) *
+                        (uint32_t)((h->dims.nz + zslab[m] - 1) / zslab[m]);
+    g.views[m].tick_blocks = g.views[C + m].tick_blocks = nt;
     g.zslab[m] = zslab[m];
   }
   if (!tiles.empty()) std::memcpy(g.tiles, tiles.data(), tiles.size() * sizeof(BatchTile));

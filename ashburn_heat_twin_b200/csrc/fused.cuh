@@ -385,7 +385,7 @@ template <class S>
 __device__ __forceinline__ void collide_store(const DomainView& D, const ParamsHead& P,
                                               const Column<RealOf<S>>& C, int k, uint32_t n,
                                               const Cell<RealOf<S>>& X,
-                                              const Macro<RealOf<S>>& M) {
+                                              const Macro<RealOf<S>>& M, uint32_t rs) {
   using R = RealOf<S>;
   using KF = CodecF<S>;
   using KG = CodecG<S>;
@@ -437,7 +437,7 @@ __device__ __forceinline__ void collide_store(const DomainView& D, const ParamsH
     const R fr = w45 * (qn - trN);
     const R cF = cdot<R, cx, cy, cz>(Fx, Fy, Fz);
     const R Fq = fpre * w * (R(3.0) * (cF - uF) + R(9.0) * cu * cF);
-    KF::store(fB + (n + D.plane[q]), KF::enc_f(feq + om * fr + Fq, w));
+    KF::store(fB + (n + D.plane[q]), enc_f_d<KF>(feq + om * fr + Fq, w, rs));
   });
   R Ssrc = R(0);
   if (k == C.kg) Ssrc = R(C.qsrc) * R(P.srcscale);
@@ -447,7 +447,7 @@ __device__ __forceinline__ void collide_store(const DomainView& D, const ParamsH
     constexpr int cx = kC7[q][0], cy = kC7[q][1], cz = kC7[q][2];
     const R w = R(w7(q));
     const R geq = w * M.th * (R(1.0) + R(4.0) * cdot<R, cx, cy, cz>(ux, uy, uz));
-    KG::store(gB + (n + D.plane[q]), KG::enc_g((X.g[q] + omg * (geq - X.g[q]) + w * Ssrc) * (R(1.0) - M.sg)));
+    KG::store(gB + (n + D.plane[q]), enc_g_d<KG>((X.g[q] + omg * (geq - X.g[q]) + w * Ssrc) * (R(1.0) - M.sg), rs));
   });
 }
 
@@ -472,7 +472,7 @@ template <class S>
 __device__ __forceinline__ void fast_update(const DomainView& D, const ParamsHead& P,
                                             const Column<RealOf<S>>& C, int k, uint32_t n,
                                             const Cell<RealOf<S>>& X,
-                                            Macro<RealOf<S>>& M) {
+                                            Macro<RealOf<S>>& M, uint32_t rs) {
   using R = RealOf<S>;
   using KF = CodecF<S>;
   using KG = CodecG<S>;
@@ -499,11 +499,11 @@ __device__ __forceinline__ void fast_update(const DomainView& D, const ParamsHea
       P, m, X.g, X.uI, X.vI, X.kb, sg, Fx0, Fy0, Ssrc, tb_add, o,
       [&](auto Q, R v) {
         constexpr int q = Q;
-        KF::store(static_cast<StoreF<S>*>(D.dst_f[q]) + n, KF::enc_f(v, R(w19(q))));
+        KF::store(static_cast<StoreF<S>*>(D.dst_f[q]) + n, enc_f_d<KF>(v, R(w19(q)), rs));
       },
       [&](auto Q, R v) {
         constexpr int q = Q;
-        KG::store(static_cast<StoreG<S>*>(D.dst_g[q]) + n, KG::enc_g(v));
+        KG::store(static_cast<StoreG<S>*>(D.dst_g[q]) + n, enc_g_d<KG>(v, rs));
       });
   M.rho = m.rho;
   M.jx = m.jx;
@@ -537,9 +537,15 @@ __device__ __forceinline__ float2 pair_load_g(const T* p, uint32_t ps) {
     return make_float2(K::load(p), K::load(p + ps));
 }
 template <class T>
-__device__ __forceinline__ void pair_store_f(T* p, uint32_t ps, float2 v, float w) {
+__device__ __forceinline__ void pair_store_f(T* p, uint32_t ps, float2 v, float w, uint32_t& r0, uint32_t& r1) {
   using K = Codec<T>;
-  if constexpr (K::kBytes == 2) {
+  if constexpr (K::kDither) {
+    const float2 e = vfma(v, vc<float2>(K::kF), vc<float2>(-(double)K::kF * w));
+    r0 = lcg_next(r0);
+    r1 = lcg_next(r1);
+    K::store(p, K::cvt_sr(e.x, r0));
+    K::store(p + ps, K::cvt_sr(e.y, r1));
+  } else if constexpr (K::kBytes == 2) {
     const float2 e = vfma(v, vc<float2>(K::kF), vc<float2>(-(double)K::kF * w));
     K::store(p, K::cvt(e.x));
     K::store(p + ps, K::cvt(e.y));
@@ -549,9 +555,15 @@ __device__ __forceinline__ void pair_store_f(T* p, uint32_t ps, float2 v, float 
   }
 }
 template <class T>
-__device__ __forceinline__ void pair_store_g(T* p, uint32_t ps, float2 v) {
+__device__ __forceinline__ void pair_store_g(T* p, uint32_t ps, float2 v, uint32_t& r0, uint32_t& r1) {
   using K = Codec<T>;
-  if constexpr (K::kBytes == 2) {
+  if constexpr (K::kDither) {
+    const float2 e = vmul(v, vc<float2>(K::kG));
+    r0 = lcg_next(r0);
+    r1 = lcg_next(r1);
+    K::store(p, K::cvt_sr(e.x, r0));
+    K::store(p + ps, K::cvt_sr(e.y, r1));
+  } else if constexpr (K::kBytes == 2) {
     const float2 e = vmul(v, vc<float2>(K::kG));
     K::store(p, K::cvt(e.x));
     K::store(p + ps, K::cvt(e.y));
@@ -566,7 +578,7 @@ __device__ __forceinline__ void pair_store_g(T* p, uint32_t ps, float2 v) {
 // bit-identical to stream_interior + fast_update on that cell alone.
 template <class S>
 __device__ __forceinline__ void fast_pair(const DomainView& D, const ParamsHead& P, const float4* prof,
-                                          const Column<float>& C, int k, uint32_t n) {
+                                          const Column<float>& C, int k, uint32_t n, uint32_t r0, uint32_t r1) {
   const StoreF<S>* fA = static_cast<const StoreF<S>*>(D.fA);
   const StoreG<S>* gA = static_cast<const StoreG<S>*>(D.gA);
   StoreF<S>* fB = static_cast<StoreF<S>*>(D.fB);
@@ -593,11 +605,11 @@ __device__ __forceinline__ void fast_pair(const DomainView& D, const ParamsHead&
       make_float2(sponge_sg(P, D.nz, k), sponge_sg(P, D.nz, k + 1)), zero, zero, zero, tb_add, o,
       [&](auto Q, float2 v) {
         constexpr int q = Q;
-        pair_store_f(static_cast<StoreF<S>*>(D.dst_f[q]) + n, ps, v, (float)w19(q));
+        pair_store_f(static_cast<StoreF<S>*>(D.dst_f[q]) + n, ps, v, (float)w19(q), r0, r1);
       },
       [&](auto Q, float2 v) {
         constexpr int q = Q;
-        pair_store_g(static_cast<StoreG<S>*>(D.dst_g[q]) + n, ps, v);
+        pair_store_g(static_cast<StoreG<S>*>(D.dst_g[q]) + n, ps, v, r0, r1);
       });
 }
 
@@ -620,6 +632,11 @@ __device__ __forceinline__ void step_block(const DomainView& D, int bx, int by, 
   if (tid < 16) reinterpret_cast<int*>(&sP)[tid] = reinterpret_cast<const int*>(D.params)[tid];
   const float4* gprof = reinterpret_cast<const float4*>(D.params + 64);
   for (int z = tid; z < D.nz; z += nthr) smem_prof[z] = gprof[z];
+  // stochastic rounding: the step counter keys this step's dithers (read before the block reports done, so every
+  // block of a step sees the same value)
+  __shared__ uint32_t s_tkey;
+  if constexpr (kDitherOf<S>)
+    if (tid == 0) s_tkey = mix32(__ldcg(D.tick) * 0x9e3779b9u + 0x632be5abu);
   __syncthreads();
   const ParamsHead& P = sP;
 
@@ -645,6 +662,17 @@ __device__ __forceinline__ void step_block(const DomainView& D, int bx, int by, 
   }
   const int kw = __reduce_min_sync(0xffffffffu, kstart);
   const uint32_t base = (uint32_t)j * (uint32_t)D.px + (uint32_t)i;
+  // dither seed of the cell at level k: its index in the whole domain (so y-slabs draw the dithers of the undivided
+  // domain) mixed with the step key
+  uint32_t gid0 = 0, gstep = 0;
+  if constexpr (kDitherOf<S>) {
+    gid0 = (uint32_t)(j + D.jg0) * (uint32_t)D.px + (uint32_t)i;
+    gstep = (uint32_t)D.nyg * (uint32_t)D.px;
+  }
+  auto seed = [&](int kk) -> uint32_t {
+    if constexpr (kDitherOf<S>) return mix32((gid0 + (uint32_t)kk * gstep) ^ s_tkey);
+    else return 0u;
+  };
   // PAIRS (FMA build without output modes): two interior levels at a time on the packed f32x2 lanes when every
   // active lane of the warp has both cells interior (bit-identical to the single-level path; more registers)
   constexpr bool kPairs = PAIRS && FAST && MODE == 0 && !BUDGET && std::is_same_v<R, float>;
@@ -655,7 +683,7 @@ __device__ __forceinline__ void step_block(const DomainView& D, int bx, int by, 
         const bool in2 = valid && k >= C.kg && !C.face && k >= C.kint && k + 1 < D.nz - 1;
         const unsigned m2 = __ballot_sync(0xffffffffu, valid && k + 1 >= C.kg);
         if (m2 != 0u && __ballot_sync(0xffffffffu, in2) == m2) {
-          if (in2) fast_pair<S>(D, P, smem_prof, C, k, (uint32_t)k * D.ps + base);
+          if (in2) fast_pair<S>(D, P, smem_prof, C, k, (uint32_t)k * D.ps + base, seed(k), seed(k + 1));
           ++k;
           continue;
         }
@@ -672,10 +700,10 @@ __device__ __forceinline__ void step_block(const DomainView& D, int bx, int by, 
       else stream_cell<S>(D, P, smem_prof, C, k, n, X);
       Macro<R> M;
       if constexpr (FAST) {
-        fast_update<S>(D, P, C, k, n, X, M);
+        fast_update<S>(D, P, C, k, n, X, M, seed(k));
       } else {
         moments_forces<R>(P, C, k, D.nz, X, M);
-        collide_store<S>(D, P, C, k, n, X, M);
+        collide_store<S>(D, P, C, k, n, X, M, seed(k));
       }
       if constexpr (MODE == 1) {
         D.dbg[n] = make_float4((float)M.th, (float)M.ux, (float)M.uy, (float)M.uz);

@@ -60,6 +60,7 @@ struct Codec;
 template <>
 struct Codec<float> {
   using Real = float;
+  static constexpr bool kDither = false;
   static constexpr int kBytes = 4;
   __device__ __forceinline__ static float load(const float* p) { return __ldg(p); }
   __device__ __forceinline__ static void store(float* p, float v) { __stcs(p, v); }
@@ -72,6 +73,7 @@ struct Codec<float> {
 template <>
 struct Codec<double> {
   using Real = double;
+  static constexpr bool kDither = false;
   static constexpr int kBytes = 8;
   __device__ __forceinline__ static double load(const double* p) { return __ldg(p); }
   __device__ __forceinline__ static void store(double* p, double v) { __stcs(p, v); }
@@ -86,6 +88,7 @@ struct Codec<double> {
 template <>
 struct Codec<__half> {
   using Real = float;
+  static constexpr bool kDither = false;
   static constexpr int kBytes = 2;
   // 16-bit traffic goes through the unsigned short load / store builtins (the __half overloads are inline-asm
   // wrappers the scheduler cannot reason about)
@@ -112,6 +115,7 @@ struct Codec<__half> {
 template <>
 struct Codec<__nv_bfloat16> {
   using Real = float;
+  static constexpr bool kDither = false;
   static constexpr int kBytes = 2;
   __device__ __forceinline__ static __nv_bfloat16 load(const __nv_bfloat16* p) {
     return __ushort_as_bfloat16(__ldg(reinterpret_cast<const unsigned short*>(p)));
@@ -136,6 +140,80 @@ struct Codec<__nv_bfloat16> {
   __device__ __forceinline__ static float raw(__nv_bfloat16 v) { return __bfloat162float(v); }
   __device__ __forceinline__ static __nv_bfloat16 cvt(float v) { return __float2bfloat16_rn(v); }
 };
+
+// FP16 storage whose step stores round stochastically: the same bits in memory as the __half codec ((f - w) * 16
+// and g * 16), decoded alike, but the fused step encodes each population by adding a pseudo-random 13-bit dither below
+// the 13 mantissa bits an f32 -> f16 conversion drops and truncating, so a value rounds up with probability equal to
+// the dropped fraction (unbiased in the f16 normal range; below 2^-14 the dither covers only part of the dropped bits
+// and rounding leans toward zero). Round-to-nearest keeps a quasi-steady state's rounding error the same step after
+// step, a persistent bias the flow integrates; the dither makes it zero-mean noise. Conversions outside the step (state
+// upload, initialisation) round to nearest like the __half codec.
+struct half_sr {
+  unsigned short x;
+};
+template <>
+struct Codec<half_sr> {
+  using Real = float;
+  static constexpr bool kDither = true;
+  static constexpr int kBytes = 2;
+  __device__ __forceinline__ static half_sr load(const half_sr* p) {
+    return half_sr{__ldg(reinterpret_cast<const unsigned short*>(p))};
+  }
+  __device__ __forceinline__ static void store(half_sr* p, half_sr v) {
+    __stcs(reinterpret_cast<unsigned short*>(p), v.x);
+  }
+  __device__ __forceinline__ static float raw(half_sr v) { return __half2float(__ushort_as_half(v.x)); }
+  __device__ __forceinline__ static half_sr cvt(float v) { return half_sr{__half_as_ushort(__float2half_rn(v))}; }
+  // r: 32 pseudo-random bits, of which the top 13 are the dither
+  __device__ __forceinline__ static half_sr cvt_sr(float v, uint32_t r) {
+    return half_sr{__half_as_ushort(__float2half_rz(__uint_as_float(__float_as_uint(v) + (r >> 19))))};
+  }
+  __device__ __forceinline__ static float dec_f(half_sr v, float w) { return __fmaf_rn(raw(v), 1.0f / kScaleF16, w); }
+  __device__ __forceinline__ static float dec_g(half_sr v) { return __fmul_rn(raw(v), 1.0f / kScaleG16); }
+  __device__ __forceinline__ static half_sr enc_f(float v, float w) {
+    return cvt(__fmaf_rn(v, kScaleF16, -kScaleF16 * w));
+  }
+  __device__ __forceinline__ static half_sr enc_g(float v) { return cvt(__fmul_rn(v, kScaleG16)); }
+  __device__ __forceinline__ static half_sr enc_f_sr(float v, float w, uint32_t r) {
+    return cvt_sr(__fmaf_rn(v, kScaleF16, -kScaleF16 * w), r);
+  }
+  __device__ __forceinline__ static half_sr enc_g_sr(float v, uint32_t r) { return cvt_sr(__fmul_rn(v, kScaleG16), r); }
+  static constexpr float kF = kScaleF16, kG = kScaleG16;
+};
+
+// Dither stream of one cell update: seeded from the cell's global index and the step counter through a 32-bit
+// integer finaliser (the "lowbias32" xorshift-multiply hash published by C. Wellons), then one step of a 32-bit
+// linear congruential generator per stored population (multiplier and increment of the PCG family's 32-bit LCG; the
+// top bits are used).
+__host__ __device__ __forceinline__ uint32_t mix32(uint32_t x) {
+  x ^= x >> 16;
+  x *= 0x7feb352du;
+  x ^= x >> 15;
+  x *= 0x846ca68bu;
+  x ^= x >> 16;
+  return x;
+}
+__host__ __device__ __forceinline__ uint32_t lcg_next(uint32_t s) { return s * 747796405u + 2891336453u; }
+
+// encode through a codec, drawing the next dither of the stream s when the codec rounds stochastically
+template <class K, class R>
+__device__ __forceinline__ auto enc_f_d(R v, R w, uint32_t& s) {
+  if constexpr (K::kDither) {
+    s = lcg_next(s);
+    return K::enc_f_sr(v, w, s);
+  } else {
+    return K::enc_f(v, w);
+  }
+}
+template <class K, class R>
+__device__ __forceinline__ auto enc_g_d(R v, uint32_t& s) {
+  if constexpr (K::kDither) {
+    s = lcg_next(s);
+    return K::enc_g_sr(v, s);
+  } else {
+    return K::enc_g(v);
+  }
+}
 
 // Storage of a state: a plain type stores f and g alike; Mixed<SF, SG> stores the flow populations f as SF and the
 // temperature populations g as SG (16-bit f with f32 g keeps the heat budget: a per-step source increment can be
@@ -162,6 +240,9 @@ template <class S>
 using StoreF = typename StorageOf<S>::F;
 template <class S>
 using StoreG = typename StorageOf<S>::G;
+// whether the step's stores of storage S draw dithers (and so read and advance the step counter)
+template <class S>
+inline constexpr bool kDitherOf = Codec<typename StorageOf<S>::F>::kDither || Codec<typename StorageOf<S>::G>::kDither;
 
 // Parameter block (kernel.js:44-50): 16 four-byte scalars, then nz x float4 (uin, vin, kbg, 0)
 struct ParamsHead {
@@ -190,6 +271,10 @@ struct DomainView {
   double* sacc;
   double* facc;
   int* err;                     // error word: a staged copy that did not arrive in time sets it
+  // stochastic-rounding storages: [0] steps taken (seeds the dithers), [1] blocks (tiles) of the current step done;
+  // the last block of a step to finish advances [0]. tick_blocks: blocks (tiles) of one step in a batched launch
+  uint32_t* tick;
+  uint32_t tick_blocks;
   int nx, ny, nz, px;
   // y-slab of a larger domain: local row 0 is global row jg0 of nyg; only local rows [jlo, jhi) are updated (the
   // others are ghost rows refreshed from the neighbouring slabs); a whole domain has jg0 0, nyg ny, [0, ny)

@@ -18,9 +18,21 @@ namespace AHX_STEP_NS {
 
 // MINB = 0: up to 256 threads per block, registers as the compiler likes; MINB = 4 / 5 / 6: 128-thread blocks with
 // 4 / 5 / 6 resident per SM (a 128 / 96 / 80 register budget), chosen by the launch-shape tuner
+// Stochastic-rounding storages: a block (tile) of a step reports done; the last of the step's `blocks` to do so
+// advances the step counter the next step's dithers are keyed on (every block read it before reporting).
+__device__ __forceinline__ void tick_done(const DomainView& D, uint32_t blocks) {
+  if (threadIdx.x == 0 && threadIdx.y == 0) {
+    if (atomicAdd(D.tick + 1, 1u) == blocks - 1) {
+      atomicExch(D.tick + 1, 0u);
+      atomicAdd(D.tick, 1u);
+    }
+  }
+}
+
 template <class S, int MODE, bool BUDGET, int MINB, bool PAIRS = false>
 __global__ void __launch_bounds__(MINB ? 128 : 256, MINB ? MINB : 1) step_kernel(DomainView D, int zslab) {
   step_block<S, MODE, BUDGET, AHX_STEP_FAST != 0, PAIRS>(D, blockIdx.x, blockIdx.y, blockIdx.z, zslab);
+  if constexpr (kDitherOf<S>) tick_done(D, gridDim.x * gridDim.y * gridDim.z);
 }
 
 template <class S, int TY, int DEPTH>
@@ -57,6 +69,7 @@ __global__ void __launch_bounds__(128, MINB) batch_kernel(const DomainView* __re
     if (tid == 0) s_zslab = zslabs[T.member];
     __syncthreads();
     step_block<S, 0, false, AHX_STEP_FAST != 0, PAIRS>(sD, T.bx, T.by, T.bz, s_zslab);
+    if constexpr (kDitherOf<S>) tick_done(sD, sD.tick_blocks);
     __syncthreads();   // the next tile overwrites the view, the staged profile and s_t
   }
   if (tid == 0) {
@@ -102,6 +115,7 @@ cudaError_t launch_batch(const BatchLaunch& B, cudaStream_t s, int* occupancy) {
     case 3: return batch_s<double>(B, s, occupancy);
     case 4: return batch_s<Mixed<__half, float>>(B, s, occupancy);
     case 5: return batch_s<Mixed<__nv_bfloat16, float>>(B, s, occupancy);
+    case 6: return batch_s<half_sr>(B, s, occupancy);
     default: return cudaErrorInvalidValue;
   }
 }
@@ -141,8 +155,8 @@ static cudaError_t launch_tma(const DomainView& D, const StepLaunch& L, cudaStre
 
 template <class S, int MODE, bool BUDGET>
 static cudaError_t launch_t(const DomainView& D, const StepLaunch& L, cudaStream_t s) {
-  if constexpr (MODE == 0 && !BUDGET && std::is_same_v<StoreF<S>, StoreG<S>>) {
-    // the staged kernel stages f and g with one element size: uniform storages only
+  if constexpr (MODE == 0 && !BUDGET && std::is_same_v<StoreF<S>, StoreG<S>> && !kDitherOf<S>) {
+    // the staged kernel stages f and g with one element size: uniform round-to-nearest storages only
     if (L.tma_ty > 0 && L.maps != nullptr) return launch_tma<S>(D, L, s);
   }
   const int minb = (MODE == 0 && !BUDGET) ? L.minb : 0;
@@ -203,6 +217,7 @@ cudaError_t launch_step(const DomainView& D, const StepLaunch& L, cudaStream_t s
     case 3: return launch_s<double>(D, L, s);
     case 4: return launch_s<Mixed<__half, float>>(D, L, s);
     case 5: return launch_s<Mixed<__nv_bfloat16, float>>(D, L, s);
+    case 6: return launch_s<half_sr>(D, L, s);
     default: return cudaErrorInvalidValue;
   }
 }

@@ -161,6 +161,7 @@ constexpr size_t tma_smem_bytes(int nz) {
 
 template <class S, bool FAST, int TY, int DEPTH>
 __device__ __forceinline__ void step_tma_block(const DomainView& D, const TmaMaps& M, int zslab) {
+  static_assert(!kDitherOf<S>, "the staged kernel takes no dither (stochastic-rounding storages use the plain kernel)");
   using R = typename Codec<S>::Real;
   using G = TmaGeom<S>;
   constexpr int STAGE = G::template stage_bytes<TY>();
@@ -227,10 +228,10 @@ __device__ __forceinline__ void step_tma_block(const DomainView& D, const TmaMap
       }
       Macro<R> Mc;
       if constexpr (FAST) {
-        fast_update<S>(D, P, C, k, n, X, Mc);
+        fast_update<S>(D, P, C, k, n, X, Mc, 0u);
       } else {
         moments_forces<R>(P, C, k, D.nz, X, Mc);
-        collide_store<S>(D, P, C, k, n, X, Mc);
+        collide_store<S>(D, P, C, k, n, X, Mc, 0u);
       }
     }
     __syncthreads();   // stage s consumed by every thread

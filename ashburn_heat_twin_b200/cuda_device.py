@@ -13,7 +13,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, 'libahx.so')
 
-PRECISIONS = {'fp32': 0, 'fp16': 1, 'bf16': 2, 'fp64': 3, 'fp16g32': 4, 'bf16g32': 5}
+PRECISIONS = {'fp32': 0, 'fp16': 1, 'bf16': 2, 'fp64': 3, 'fp16g32': 4, 'bf16g32': 5, 'fp16sr': 6}
 ARITH = {'exact': 0, 'fast': 1}
 STATUS = {0: 'AHX_OK', 1: 'AHX_EINVAL', 2: 'AHX_ENOMEM', 3: 'AHX_EDESTROYED', 4: 'AHX_EDEVICE', 5: 'AHX_ETIMEOUT',
           6: 'AHX_ENONFINITE', 7: 'AHX_EBUSY'}

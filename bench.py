@@ -62,9 +62,10 @@ WORKLOADS = {
 }
 METRIC = 'GLUPS (all cells) of the fused D3Q19+D3Q7 step, 600x600x64'
 # algorithmic bytes per fluid-cell update: read + write of 19 f and 7 g populations at their storage widths
-CELL_BYTES = {'fp32': 208, 'fp16': 104, 'bf16': 104, 'fp64': 416, 'fp16g32': 132, 'bf16g32': 132}
+CELL_BYTES = {'fp32': 208, 'fp16': 104, 'bf16': 104, 'fp64': 416, 'fp16g32': 132, 'bf16g32': 132, 'fp16sr': 104}
 DTYPE = {'fp32': 'f32', 'fp16': 'f16-store/f32', 'bf16': 'bf16-store/f32', 'fp64': 'f64',
-         'fp16g32': 'f16-store f, f32-store g / f32', 'bf16g32': 'bf16-store f, f32-store g / f32'}
+         'fp16g32': 'f16-store f, f32-store g / f32', 'bf16g32': 'bf16-store f, f32-store g / f32',
+         'fp16sr': 'f16-store (stochastic rounding) / f32'}
 
 
 def log(*a):
@@ -431,8 +432,13 @@ def main_precision(a, rank, world, local, dist, torch):
     import numpy as np
 
     from ashburn_heat_twin_b200 import params as PM
-    order = ['fp64', 'fp32', 'fp16', 'bf16', 'fp16g32', 'bf16g32']
+    order = ['fp64', 'fp32', 'fp16', 'bf16', 'fp16g32', 'bf16g32', 'fp16sr']
     sol = {p: make_solver(device=local, precision=p, arith='exact' if p == 'fp64' else 'fast') for p in order}
+    # sensitivity of the window means: FP64 runs whose flow populations get one seeded relative kick of size eps at
+    # the end of the spin-up (the size of an f32 / a 16-bit rounding), nothing else changed
+    kicks = {f'fp64 kick {e:g}': e for e in (a.kicks or ())}
+    for p in kicks:
+        sol[p] = make_solver(device=local, precision='fp64', arith='exact')
     s0 = sol['fp64']
     nx, ny, nz = s0.info['nx'], s0.info['ny'], s0.info['nz']
     N = nx * ny * nz
@@ -443,11 +449,18 @@ def main_precision(a, rank, world, local, dist, torch):
     cols = np.nonzero(ktop < nz)[0]
     fluid = (np.arange(nz)[:, None] >= ktop[None, :]).reshape(-1)
     res = {}
-    for p in order:
+    for p in order + list(kicks):
         s = sol[p]
         dev = s._dev
         t0 = time.perf_counter()
         s.step(spin).result()
+        if p in kicks:
+            f, g = dev.read_state_f64()
+            rng = np.random.default_rng(11)
+            f = f.reshape(19, N)
+            f[:, fluid] *= 1.0 + kicks[p] * rng.uniform(-1.0, 1.0, (19, int(fluid.sum())))
+            dev.write_state_f64(f, g)
+            del f, g
         st0 = dev.stats()
         dev.budget_enable(True)
         dev.budget_read(reset=True)
@@ -478,6 +491,11 @@ def main_precision(a, rank, world, local, dist, torch):
 
     def rel_l2(x, y):
         return float(np.linalg.norm(x - y) / np.linalg.norm(y))
+
+    sensitivity = {p: dict(kick=e, mean_ng_theta_rel_l2_vs_fp64=rel_l2(res[p]['ng'], ref['ng']),
+                           peak_mean_warming_k=res[p]['peak']) for p, e in kicks.items()}
+    for p in kicks:
+        sol.pop(p).destroy()
 
     # one step from the FP64 state in every storage (theta of the fluid cells)
     f64, g64 = s0._dev.read_state_f64()
@@ -519,7 +537,8 @@ def main_precision(a, rank, world, local, dist, torch):
                config=dict(workload=WORKLOADS['c3']['desc'], spin_steps=spin, mean_steps=mean, dt_s=dt,
                            near_ground='first fluid cell of each column, mean over the window',
                            parallelism=f'replicas x{world}'),
-               precision=prec, roofline=None, cpu_baseline=None, e2e=None, gpu_launches=a.steps)
+               precision=prec, sensitivity=sensitivity or None, roofline=None, cpu_baseline=None, e2e=None,
+               gpu_launches=a.steps)
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
@@ -553,6 +572,8 @@ def main():
     ap.add_argument('--chunk', type=int, default=64, help='serving: steps per batched chunk')
     ap.add_argument('--spin-s', type=float, default=120.0, help='precision study: simulated spin-up seconds')
     ap.add_argument('--mean-s', type=float, default=600.0, help='precision study: simulated averaging seconds')
+    ap.add_argument('--kicks', type=float, nargs='*', default=None,
+                    help='precision study: also run FP64 with one relative kick of each size after the spin-up')
     a = ap.parse_args()
     a.warmup = max(a.warmup, 3)
 

@@ -39,14 +39,17 @@ typedef enum {
 
 /* storage of the populations (arithmetic is f32, f64 for AHX_FP64). The 16-bit formats store (f - w) * scale for the
  * flow populations; AHX_FP16_G32 / AHX_BF16_G32 store f in 16 bits and the temperature populations g in f32, which
- * keeps the heat budget (a per-step source increment can be far below half an ulp of a 16-bit g). */
+ * keeps the heat budget (a per-step source increment can be far below half an ulp of a 16-bit g). AHX_FP16_SR is
+ * the AHX_FP16 format whose step rounds stochastically (a dither keyed on the cell and a per-handle step counter,
+ * deterministic for a given history): unbiased rounding instead of round-to-nearest's persistent bias. */
 typedef enum {
   AHX_FP32 = 0,
   AHX_FP16 = 1,
   AHX_BF16 = 2,
   AHX_FP64 = 3,
   AHX_FP16_G32 = 4,
-  AHX_BF16_G32 = 5
+  AHX_BF16_G32 = 5,
+  AHX_FP16_SR = 6
 } ahx_precision;
 
 /* step output modes (kernel.js:427-428; solver.js:551-558 stepOut / stepAcc) */

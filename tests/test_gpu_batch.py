@@ -40,7 +40,8 @@ def same(a, b):
     assert np.array_equal(fa, fb) and np.array_equal(ga, gb)
 
 
-@pytest.mark.parametrize('precision,arith', [('fp32', 'exact'), ('fp32', 'fast'), ('fp16', 'fast')])
+@pytest.mark.parametrize('precision,arith', [('fp32', 'exact'), ('fp32', 'fast'), ('fp16', 'fast'),
+                                            ('fp16sr', 'fast')])
 def test_batch_matches_solo(precision, arith):
     solo = [scenario(i, precision, arith) for i in range(3)]
     mem = [scenario(i, precision, arith) for i in range(3)]

@@ -143,7 +143,8 @@ def test_fp64_build_bit_exact_with_fp64_oracle():
     o.destroy()
 
 
-@pytest.mark.parametrize('precision,tol', [('fp16', 2e-3), ('bf16', 2e-2), ('fp16g32', 2e-3), ('bf16g32', 2e-2)])
+@pytest.mark.parametrize('precision,tol', [('fp16', 2e-3), ('bf16', 2e-2), ('fp16g32', 2e-3), ('bf16g32', 2e-2),
+                                           ('fp16sr', 2e-3)])
 def test_16bit_storage_error_vs_fp64(precision, tol):
     """16-bit population storage (f shifted by w_q and scaled; g likewise, or f32 for the *g32 storages) against
     the FP64 build after 300 steps with heat on: theta rel-L2 over fluid cells within the stated tolerance."""
@@ -213,7 +214,7 @@ def test_launch_shapes_bit_exact(shape, zslab):
     o.destroy()
 
 
-@pytest.mark.parametrize('precision', ['fp32', 'fp16', 'fp16g32'])
+@pytest.mark.parametrize('precision', ['fp32', 'fp16', 'fp16g32', 'fp16sr'])
 def test_paired_levels_bit_identical(precision):
     """The FMA build's paired path (two interior levels per thread on packed f32x2 arithmetic, launch shapes
     2404 / 2504 / 2604) leaves exactly the state and outputs of the unpaired path, with whole columns and with odd

@@ -18,7 +18,7 @@ def opts():
 
 
 @pytest.mark.parametrize('nslabs,precision,arith', [(2, 'fp32', 'exact'), (3, 'fp32', 'exact'), (3, 'fp32', 'fast'),
-                                                    (2, 'fp16', 'fast')])
+                                                    (2, 'fp16', 'fast'), (3, 'fp16sr', 'fast')])
 def test_slabs_match_the_undivided_domain(nslabs, precision, arith):
     whole = S.create_live_solver(backend=cuda_backend(precision, arith), **opts())
     sd = SlabDomain(nslabs, precision=precision, arith=arith, **opts())
