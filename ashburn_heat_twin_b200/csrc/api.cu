@@ -449,7 +449,7 @@ ahx_status ahx_set_parity(ahx_handle* h, int parity) {
 }
 
 // Everything a plain step's launches depend on besides the parity (buffers and tables are fixed per handle).
-uint64_t launch_key(const ahx_handle* h, const StepLaunch& L) {
+static uint64_t launch_key(const ahx_handle* h, const StepLaunch& L) {
   uint64_t k = 1469598103934665603ull;
   const int v[] = {L.precision, L.block_y, L.zslab, L.minb, (int)L.pairs, L.tma_ty, L.tma_depth,
                    h->jg0, h->nyg, h->jlo, h->jhi, h->dims.arith};
@@ -459,7 +459,7 @@ uint64_t launch_key(const ahx_handle* h, const StepLaunch& L) {
 
 // two plain steps starting at parity p, captured once per launch set-up and replayed (launch gaps matter for small
 // grids, where a step takes tens of microseconds)
-ahx_status step_graph(ahx_handle* h, const StepLaunch& L0, int p, cudaGraphExec_t* out) {
+static ahx_status step_graph(ahx_handle* h, const StepLaunch& L0, int p, cudaGraphExec_t* out) {
   const uint64_t key = launch_key(h, L0);
   if (h->graph[p] && h->graph_key[p] == key) {
     *out = h->graph[p];
@@ -495,14 +495,8 @@ ahx_status step_graph(ahx_handle* h, const StepLaunch& L0, int p, cudaGraphExec_
   return AHX_OK;
 }
 
-ahx_status ahx_step(ahx_handle* h, int n, int mode) {
-  if (!h) return fail(AHX_EINVAL, "live solver: null handle");
-  std::lock_guard<std::mutex> lk(h->mu);
-  if (ahx_status st = check(h)) return st;
-  if (n < 0 || mode < 0 || mode > 2) return fail(AHX_EINVAL, "live solver: bad step count or mode");
-  AHX_CUDA(h, cudaSetDevice(h->dev));
-  if (mode != AHX_MODE_NONE)
-    if (ahx_status st = ensure_dbg(h)) return st;
+// the launch set-up of this handle's steps (mode and tensor maps are per step)
+static StepLaunch step_launch(const ahx_handle* h) {
   StepLaunch L;
   L.precision = h->dims.precision;
   L.budget = h->budget_on || h->accum_on;
@@ -512,8 +506,25 @@ ahx_status ahx_step(ahx_handle* h, int n, int mode) {
   L.pairs = h->pairs;
   L.tma_ty = h->maps_ok ? h->tma_ty : 0;
   L.tma_depth = h->tma_depth;
+  return L;
+}
+
+// whether n steps in this mode replay the two-step graph
+static bool graph_steps(const ahx_handle* h, int n, int mode) {
+  return mode == AHX_MODE_NONE && !(h->budget_on || h->accum_on) && n >= 2;
+}
+
+ahx_status ahx_step(ahx_handle* h, int n, int mode) {
+  if (!h) return fail(AHX_EINVAL, "live solver: null handle");
+  std::lock_guard<std::mutex> lk(h->mu);
+  if (ahx_status st = check(h)) return st;
+  if (n < 0 || mode < 0 || mode > 2) return fail(AHX_EINVAL, "live solver: bad step count or mode");
+  AHX_CUDA(h, cudaSetDevice(h->dev));
+  if (mode != AHX_MODE_NONE)
+    if (ahx_status st = ensure_dbg(h)) return st;
+  StepLaunch L = step_launch(h);
   int s = 0;
-  if (mode == AHX_MODE_NONE && !L.budget && n >= 2) {
+  if (graph_steps(h, n, mode)) {
     // pairs of plain steps from the captured graph of the current parity
     cudaGraphExec_t g = nullptr;
     if (ahx_status st = step_graph(h, L, h->parity, &g)) return st;
@@ -543,6 +554,11 @@ ahx_status ahx_time_steps(ahx_handle* h, int n, int mode, int timeout_ms, float*
     std::lock_guard<std::mutex> lk(h->mu);
     if (ahx_status st = check(h)) return st;
     AHX_CUDA(h, cudaSetDevice(h->dev));
+    if (n < 0 || mode < 0 || mode > 2) return fail(AHX_EINVAL, "live solver: bad step count or mode");
+    if (graph_steps(h, n, mode)) {   // capture outside the timed region
+      cudaGraphExec_t g = nullptr;
+      if (ahx_status st = step_graph(h, step_launch(h), h->parity, &g)) return st;
+    }
     AHX_CUDA(h, cudaEventCreate(&e0));
     AHX_CUDA(h, cudaEventCreate(&e1));
     AHX_CUDA(h, cudaEventRecord(e0, h->s_step));
