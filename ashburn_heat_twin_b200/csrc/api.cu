@@ -427,6 +427,8 @@ ahx_status ahx_init_flow(ahx_handle* h) {
   AHX_CUDA(h, cudaSetDevice(h->dev));
   DomainView D = view(h);
   AHX_CUDA(h, launch_init(D, h->dims.precision, h->f[0], h->f[1], h->s_step));
+  // a re-initialised flow continues like a fresh handle: the stochastic-rounding step counter restarts too
+  AHX_CUDA(h, cudaMemsetAsync(h->d_tick, 0, 2 * sizeof(uint32_t), h->s_step));
   return AHX_OK;
 }
 

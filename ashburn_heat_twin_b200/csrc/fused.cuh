@@ -623,20 +623,23 @@ constexpr int kBlockX = 32;
 
 // The fused step over one z-slab of the columns of a block. MODE: 0 none, 1 write dbg, 2 accumulate dbg.
 template <class S, int MODE, bool BUDGET, bool FAST, bool PAIRS = false>
-__device__ __forceinline__ void step_block(const DomainView& D, int bx, int by, int bz, int zslab) {
+// stage = false: the block staged this domain's parameters, profile and step key for an earlier tile (batched step)
+__device__ __forceinline__ void step_block(const DomainView& D, int bx, int by, int bz, int zslab, bool stage = true) {
   using R = RealOf<S>;
   extern __shared__ float4 smem_prof[];
   __shared__ ParamsHead sP;
   const int tid = threadIdx.y * blockDim.x + threadIdx.x;
   const int nthr = blockDim.x * blockDim.y;
-  if (tid < 16) reinterpret_cast<int*>(&sP)[tid] = reinterpret_cast<const int*>(D.params)[tid];
-  const float4* gprof = reinterpret_cast<const float4*>(D.params + 64);
-  for (int z = tid; z < D.nz; z += nthr) smem_prof[z] = gprof[z];
   // stochastic rounding: the step counter keys this step's dithers (read before the block reports done, so every
   // block of a step sees the same value)
   __shared__ uint32_t s_tkey;
-  if constexpr (kDitherOf<S>)
-    if (tid == 0) s_tkey = mix32(__ldcg(D.tick) * 0x9e3779b9u + 0x632be5abu);
+  if (stage) {
+    if (tid < 16) reinterpret_cast<int*>(&sP)[tid] = reinterpret_cast<const int*>(D.params)[tid];
+    const float4* gprof = reinterpret_cast<const float4*>(D.params + 64);
+    for (int z = tid; z < D.nz; z += nthr) smem_prof[z] = gprof[z];
+    if constexpr (kDitherOf<S>)
+      if (tid == 0) s_tkey = mix32(__ldcg(D.tick) * 0x9e3779b9u + 0x632be5abu);
+  }
   __syncthreads();
   const ParamsHead& P = sP;
 

@@ -42,35 +42,47 @@ __global__ void __launch_bounds__(32 * TY, TY == 4 ? 4 : 2)
 }
 
 // Batched step: one persistent launch steps every member domain of a batch. Blocks take tiles (32 x 4 columns x that
-// member's z-slab) from a device counter in list order until the list is exhausted, so unequal tiles balance; each
-// tile copies its member's view to shared memory and runs the same step_block as a solo launch, so a member's
-// result is bit-identical to stepping it alone. The tile count is read from device memory, so one captured launch
-// serves any membership the tables describe. The last block to finish resets the counters for the next launch on
-// the stream (launches on one stream do not overlap).
+// member's z-slab) from a device counter in list order until the list is exhausted, so unequal tiles balance; a
+// block fetches its next tile index while it works on the current one, and copies a member's view (and stages its
+// parameters and profile) only when the tile's member differs from its previous tile's. Each tile runs the same
+// step_block as a solo launch, so a member's result is bit-identical to stepping it alone. The tile count is read
+// from device memory, so one captured launch serves any membership the tables describe. The last block to finish
+// resets the counters for the next launch on the stream (launches on one stream do not overlap).
 template <class S, int MINB, bool PAIRS>
 __global__ void __launch_bounds__(128, MINB) batch_kernel(const DomainView* __restrict__ views,
                                                           const BatchTile* __restrict__ tiles,
                                                           const int* __restrict__ zslabs,
                                                           const int* __restrict__ ntiles_ptr, int* sched) {
   __shared__ DomainView sD;
-  __shared__ int s_zslab, s_t;
+  __shared__ int s_zslab, s_t, s_member;
   static_assert(sizeof(DomainView) % 4 == 0, "the view copies as 32-bit words");
   const int tid = threadIdx.y * 32 + threadIdx.x;
   const int ntiles = *ntiles_ptr;
+  if (tid == 0) {
+    s_member = -1;
+    s_t = atomicAdd(&sched[0], 1);
+  }
+  __syncthreads();
   for (;;) {
-    if (tid == 0) s_t = atomicAdd(&sched[0], 1);
-    __syncthreads();
     const int t = s_t;
     if (t >= ntiles) break;
     const BatchTile T = tiles[t];
-    const int* src = reinterpret_cast<const int*>(views + T.member);
-    int* dst = reinterpret_cast<int*>(&sD);
-    for (int w = tid; w < (int)(sizeof(DomainView) / 4); w += 128) dst[w] = src[w];
-    if (tid == 0) s_zslab = zslabs[T.member];
+    const bool fresh = (int)T.member != s_member;
+    __syncthreads();   // every thread has read s_t and s_member
+    if (tid == 0) s_t = atomicAdd(&sched[0], 1);   // the next tile, fetched while this one runs
+    if (fresh) {
+      const int* src = reinterpret_cast<const int*>(views + T.member);
+      int* dst = reinterpret_cast<int*>(&sD);
+      for (int w = tid; w < (int)(sizeof(DomainView) / 4); w += 128) dst[w] = src[w];
+      if (tid == 0) {
+        s_zslab = zslabs[T.member];
+        s_member = T.member;
+      }
+    }
     __syncthreads();
-    step_block<S, 0, false, AHX_STEP_FAST != 0, PAIRS>(sD, T.bx, T.by, T.bz, s_zslab);
+    step_block<S, 0, false, AHX_STEP_FAST != 0, PAIRS>(sD, T.bx, T.by, T.bz, s_zslab, fresh);
     if constexpr (kDitherOf<S>) tick_done(sD, sD.tick_blocks);
-    __syncthreads();   // the next tile overwrites the view, the staged profile and s_t
+    __syncthreads();   // the next tile may overwrite the view and the staged profile
   }
   if (tid == 0) {
     __threadfence();

@@ -61,16 +61,25 @@ def _state_bytes(solver):
         return solver.info['nCells'] * 52 * 4
 
 
+# launch of the serving batch on B200 (96-register variant, 8-level tiles): the fastest of the register variants x
+# tile depths on the 40/40/20 % mix of 40 / 30 / 20 m requests
+DEFAULT_BATCH_LAUNCH = dict(minb=5, zslab=8)
+
+
 class Server:
     """Continuous-batching server on one device. `backend` builds a solver's device (CudaDevice by default);
     `batch_factory(solvers)` returns an object with step(n) -> Pending, set_members(solvers) and destroy()
-    (LiveBatch by default)."""
+    (LiveBatch by default); `batch_launch` holds its set_launch keywords (DEFAULT_BATCH_LAUNCH with LiveBatch, none
+    with another factory unless given)."""
 
     def __init__(self, static, backend=None, batch_factory=None, max_cells=64_000_000, chunk=64, u10Max=8.0,
-                 hbm_budget_bytes=None, depth=2, clock=time.perf_counter, sleep=time.sleep):
+                 hbm_budget_bytes=None, depth=2, clock=time.perf_counter, sleep=time.sleep, batch_launch=None):
         self.static = static
         self.backend = backend
         self.batch_factory = batch_factory or S.LiveBatch
+        if batch_launch is None and batch_factory is None:
+            batch_launch = DEFAULT_BATCH_LAUNCH
+        self.batch_launch = dict(batch_launch) if batch_launch else None   # LiveBatch.set_launch keywords
         self.max_cells = int(max_cells)
         self.chunk = int(chunk)
         self.depth = max(1, int(depth))
@@ -182,6 +191,8 @@ class Server:
             if not members:
                 return
             self.batch = self.batch_factory(members)
+            if self.batch_launch:
+                self.batch.set_launch(**self.batch_launch)
         else:
             self.batch.set_members(members)
         self.batch_members = members

@@ -559,12 +559,12 @@ class LiveBatch:
 
     def autotune(self, steps_per_trial=4):
         """time the register-budget variants x tile depths on the batch itself and keep the fastest. Like
-        benchmark(), the trials advance every member's state (by up to 16 x (2 + steps_per_trial) steps)."""
+        benchmark(), the trials advance every member's state (by up to 24 x (2 + steps_per_trial) steps)."""
         paired = (False, True) if self.solvers[0]._dev.arith == 'fast' and self.solvers[0]._dev.precision != 'fp64' \
             else (False,)
         best = None
         for pr in paired:
-            for minb in (4, 5):
+            for minb in (4, 5, 6):
                 for zs in (2, 4, 8, 16):
                     self._b.set_launch(minb, zs, True, pr)
                     self._b.time_steps(2)

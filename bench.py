@@ -343,7 +343,9 @@ def main_serve(a, rank, world, local, dist, torch):
     # through the same server (kernels, graph capture, read-back staging)
     # admission by free device memory (80 % of what is free now) as well as by the resident-cell budget
     free_b, _ = torch.cuda.mem_get_info(local)
-    srv = SV.Server(st, backend=backend, max_cells=a.max_cells, chunk=a.chunk, hbm_budget_bytes=int(0.8 * free_b))
+    blaunch = dict(minb=a.batch_minb, zslab=a.batch_zslab) if (a.batch_minb or a.batch_zslab) else None
+    srv = SV.Server(st, backend=backend, max_cells=a.max_cells, chunk=a.chunk, hbm_budget_bytes=int(0.8 * free_b),
+                    batch_launch=blaunch)
     per_req = sum(sh * (6000 // dx) ** 2 * round(hm / dx) for sh, dx, hm in SC.SERVE_MIX)
     for sh, dx, hm in SC.SERVE_MIX:
         tmpl = SV.Request(id=-1, arrival=0.0, dx=dx, heightM=hm, met=dict(synth.C1_MET), flux=400.0,
@@ -398,7 +400,7 @@ def main_serve(a, rank, world, local, dist, torch):
                data='synthetic (seeded terrain, buildings and request trace; no public dataset involved)',
                config=dict(workload=WORKLOADS['c5']['desc'], requests=a.requests, rate_hz=a.rate, seed=a.seed,
                            precision=a.precision, arith=a.arith, max_cells=a.max_cells, chunk=a.chunk,
-                           hbm_budget_bytes=srv.hbm_budget,
+                           hbm_budget_bytes=srv.hbm_budget, batch_launch=srv.batch_launch,
                            parallelism=f'replicas x{world}', classes=classes,
                            l2='per-step state of the admitted requests >> 126 MB L2'),
                serving=dict(latency_p50_s=stats['latency_p50_s'], latency_p99_s=stats['latency_p99_s'],
@@ -572,6 +574,8 @@ def main():
     ap.add_argument('--seed', type=int, default=5, help='serving: trace seed')
     ap.add_argument('--max-cells', type=int, default=64_000_000, help='serving: resident cell budget')
     ap.add_argument('--chunk', type=int, default=64, help='serving: steps per batched chunk')
+    ap.add_argument('--batch-minb', type=int, default=0, help='serving: batch register variant (4 / 5 / 6; 0 = default)')
+    ap.add_argument('--batch-zslab', type=int, default=0, help='serving: batch tile depth in levels (0 = default)')
     ap.add_argument('--spin-s', type=float, default=120.0, help='precision study: simulated spin-up seconds')
     ap.add_argument('--mean-s', type=float, default=600.0, help='precision study: simulated averaging seconds')
     ap.add_argument('--kicks', type=float, nargs='*', default=None,

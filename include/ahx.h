@@ -133,7 +133,7 @@ ahx_status ahx_set_ktop(ahx_handle* h, const uint32_t* ktop, const uint32_t* old
 /* --- state (solver.js:288-293, 380-398) ------------------------------------------------------------------------ */
 
 /* f -> equilibrium with the inflow profile at the local height above terrain in both buffers (kernel.js:524-553
- * genInitWGSL); theta kept */
+ * genInitWGSL); theta kept; the stochastic-rounding step counter restarts (AHX_FP16_SR) */
 ahx_status ahx_init_flow(ahx_handle* h);
 
 /* g -> 0 in both buffers (solver.js:383,394 clearBuffer) */
