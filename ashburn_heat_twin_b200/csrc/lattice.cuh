@@ -164,9 +164,10 @@ struct Codec<half_sr> {
   }
   __device__ __forceinline__ static float raw(half_sr v) { return __half2float(__ushort_as_half(v.x)); }
   __device__ __forceinline__ static half_sr cvt(float v) { return half_sr{__half_as_ushort(__float2half_rn(v))}; }
-  // r: 32 pseudo-random bits, of which the top 13 are the dither
+  // r: 32 pseudo-random bits, of which the top 13 are the dither (r >> 19, taken as the high word of r * 2^13 so the
+  // extraction and the add can be one multiply-add)
   __device__ __forceinline__ static half_sr cvt_sr(float v, uint32_t r) {
-    return half_sr{__half_as_ushort(__float2half_rz(__uint_as_float(__float_as_uint(v) + (r >> 19))))};
+    return half_sr{__half_as_ushort(__float2half_rz(__uint_as_float(__umulhi(r, 0x2000u) + __float_as_uint(v))))};
   }
   __device__ __forceinline__ static float dec_f(half_sr v, float w) { return __fmaf_rn(raw(v), 1.0f / kScaleF16, w); }
   __device__ __forceinline__ static float dec_g(half_sr v) { return __fmul_rn(raw(v), 1.0f / kScaleG16); }
