@@ -437,7 +437,7 @@ __device__ __forceinline__ void collide_store(const DomainView& D, const ParamsH
     const R fr = w45 * (qn - trN);
     const R cF = cdot<R, cx, cy, cz>(Fx, Fy, Fz);
     const R Fq = fpre * w * (R(3.0) * (cF - uF) + R(9.0) * cu * cF);
-    KF::store(fB + (n + D.plane[q]), enc_f_d<KF>(feq + om * fr + Fq, w, rs));
+    KF::store(fB + (n + D.plane[q]), enc_f_d<KF, q>(feq + om * fr + Fq, w, rs));
   });
   R Ssrc = R(0);
   if (k == C.kg) Ssrc = R(C.qsrc) * R(P.srcscale);
@@ -447,7 +447,7 @@ __device__ __forceinline__ void collide_store(const DomainView& D, const ParamsH
     constexpr int cx = kC7[q][0], cy = kC7[q][1], cz = kC7[q][2];
     const R w = R(w7(q));
     const R geq = w * M.th * (R(1.0) + R(4.0) * cdot<R, cx, cy, cz>(ux, uy, uz));
-    KG::store(gB + (n + D.plane[q]), enc_g_d<KG>((X.g[q] + omg * (geq - X.g[q]) + w * Ssrc) * (R(1.0) - M.sg), rs));
+    KG::store(gB + (n + D.plane[q]), enc_g_d<KG, q>((X.g[q] + omg * (geq - X.g[q]) + w * Ssrc) * (R(1.0) - M.sg), rs));
   });
 }
 
@@ -499,11 +499,11 @@ __device__ __forceinline__ void fast_update(const DomainView& D, const ParamsHea
       P, m, X.g, X.uI, X.vI, X.kb, sg, Fx0, Fy0, Ssrc, tb_add, o,
       [&](auto Q, R v) {
         constexpr int q = Q;
-        KF::store(static_cast<StoreF<S>*>(D.dst_f[q]) + n, enc_f_d<KF>(v, R(w19(q)), rs));
+        KF::store(static_cast<StoreF<S>*>(D.dst_f[q]) + n, enc_f_d<KF, q>(v, R(w19(q)), rs));
       },
       [&](auto Q, R v) {
         constexpr int q = Q;
-        KG::store(static_cast<StoreG<S>*>(D.dst_g[q]) + n, enc_g_d<KG>(v, rs));
+        KG::store(static_cast<StoreG<S>*>(D.dst_g[q]) + n, enc_g_d<KG, q>(v, rs));
       });
   M.rho = m.rho;
   M.jx = m.jx;
@@ -536,15 +536,13 @@ __device__ __forceinline__ float2 pair_load_g(const T* p, uint32_t ps) {
   else
     return make_float2(K::load(p), K::load(p + ps));
 }
-template <class T>
-__device__ __forceinline__ void pair_store_f(T* p, uint32_t ps, float2 v, float w, uint32_t& r0, uint32_t& r1) {
+template <int P, class T>
+__device__ __forceinline__ void pair_store_f(T* p, uint32_t ps, float2 v, float w, uint32_t h0, uint32_t h1) {
   using K = Codec<T>;
   if constexpr (K::kDither) {
     const float2 e = vfma(v, vc<float2>(K::kF), vc<float2>(-(double)K::kF * w));
-    r0 = lcg_next(r0);
-    r1 = lcg_next(r1);
-    K::store(p, K::cvt_sr(e.x, r0));
-    K::store(p + ps, K::cvt_sr(e.y, r1));
+    K::store(p, K::cvt_sr(e.x, h0 * kDitherMul<P>));
+    K::store(p + ps, K::cvt_sr(e.y, h1 * kDitherMul<P>));
   } else if constexpr (K::kBytes == 2) {
     const float2 e = vfma(v, vc<float2>(K::kF), vc<float2>(-(double)K::kF * w));
     K::store(p, K::cvt(e.x));
@@ -554,15 +552,13 @@ __device__ __forceinline__ void pair_store_f(T* p, uint32_t ps, float2 v, float 
     K::store(p + ps, v.y);
   }
 }
-template <class T>
-__device__ __forceinline__ void pair_store_g(T* p, uint32_t ps, float2 v, uint32_t& r0, uint32_t& r1) {
+template <int P, class T>
+__device__ __forceinline__ void pair_store_g(T* p, uint32_t ps, float2 v, uint32_t h0, uint32_t h1) {
   using K = Codec<T>;
   if constexpr (K::kDither) {
     const float2 e = vmul(v, vc<float2>(K::kG));
-    r0 = lcg_next(r0);
-    r1 = lcg_next(r1);
-    K::store(p, K::cvt_sr(e.x, r0));
-    K::store(p + ps, K::cvt_sr(e.y, r1));
+    K::store(p, K::cvt_sr(e.x, h0 * kDitherMul<19 + P>));
+    K::store(p + ps, K::cvt_sr(e.y, h1 * kDitherMul<19 + P>));
   } else if constexpr (K::kBytes == 2) {
     const float2 e = vmul(v, vc<float2>(K::kG));
     K::store(p, K::cvt(e.x));
@@ -605,11 +601,11 @@ __device__ __forceinline__ void fast_pair(const DomainView& D, const ParamsHead&
       make_float2(sponge_sg(P, D.nz, k), sponge_sg(P, D.nz, k + 1)), zero, zero, zero, tb_add, o,
       [&](auto Q, float2 v) {
         constexpr int q = Q;
-        pair_store_f(static_cast<StoreF<S>*>(D.dst_f[q]) + n, ps, v, (float)w19(q), r0, r1);
+        pair_store_f<q>(static_cast<StoreF<S>*>(D.dst_f[q]) + n, ps, v, (float)w19(q), r0, r1);
       },
       [&](auto Q, float2 v) {
         constexpr int q = Q;
-        pair_store_g(static_cast<StoreG<S>*>(D.dst_g[q]) + n, ps, v, r0, r1);
+        pair_store_g<q>(static_cast<StoreG<S>*>(D.dst_g[q]) + n, ps, v, r0, r1);
       });
 }
 

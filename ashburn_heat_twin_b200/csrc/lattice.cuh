@@ -182,11 +182,11 @@ struct Codec<half_sr> {
   static constexpr float kF = kScaleF16, kG = kScaleG16;
 };
 
-// Dither stream of one cell update: seeded from the cell's global index and the step counter through a 32-bit
-// integer finaliser (the "lowbias32" xorshift-multiply hash published by C. Wellons), then one step of a 32-bit
-// linear congruential generator per stored population (multiplier and increment of the PCG family's 32-bit LCG; the
-// top bits are used).
-__host__ __device__ __forceinline__ uint32_t mix32(uint32_t x) {
+// Dithers of one cell update: a 32-bit seed from the cell's global index and the step counter through an integer
+// finaliser (the "lowbias32" xorshift-multiply hash published by C. Wellons); population slot p (f: q, g: 19 + q)
+// uses the top 13 bits of seed x M_p, M_p an odd constant per slot (the finaliser of a slot number), so each dither is
+// uniform (x -> x M_p is a bijection) and the 26 products are independent instructions.
+__host__ __device__ constexpr uint32_t mix32(uint32_t x) {
   x ^= x >> 16;
   x *= 0x7feb352du;
   x ^= x >> 15;
@@ -194,26 +194,19 @@ __host__ __device__ __forceinline__ uint32_t mix32(uint32_t x) {
   x ^= x >> 16;
   return x;
 }
-__host__ __device__ __forceinline__ uint32_t lcg_next(uint32_t s) { return s * 747796405u + 2891336453u; }
+template <int P>
+inline constexpr uint32_t kDitherMul = mix32(0x2545f491u + 0x9e3779b9u * (uint32_t)P) | 1u;
 
-// encode through a codec, drawing the next dither of the stream s when the codec rounds stochastically
-template <class K, class R>
-__device__ __forceinline__ auto enc_f_d(R v, R w, uint32_t& s) {
-  if constexpr (K::kDither) {
-    s = lcg_next(s);
-    return K::enc_f_sr(v, w, s);
-  } else {
-    return K::enc_f(v, w);
-  }
+// encode through a codec, with the dither of population slot P of the cell seeded h when it rounds stochastically
+template <class K, int P, class R>
+__device__ __forceinline__ auto enc_f_d(R v, R w, uint32_t h) {
+  if constexpr (K::kDither) return K::enc_f_sr(v, w, h * kDitherMul<P>);
+  else return K::enc_f(v, w);
 }
-template <class K, class R>
-__device__ __forceinline__ auto enc_g_d(R v, uint32_t& s) {
-  if constexpr (K::kDither) {
-    s = lcg_next(s);
-    return K::enc_g_sr(v, s);
-  } else {
-    return K::enc_g(v);
-  }
+template <class K, int P, class R>
+__device__ __forceinline__ auto enc_g_d(R v, uint32_t h) {
+  if constexpr (K::kDither) return K::enc_g_sr(v, h * kDitherMul<19 + P>);
+  else return K::enc_g(v);
 }
 
 // Storage of a state: a plain type stores f and g alike; Mixed<SF, SG> stores the flow populations f as SF and the
