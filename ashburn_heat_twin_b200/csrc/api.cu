@@ -100,6 +100,40 @@ size_t params_bytes(const ahx_handle* h) { return 64 + 16 * (size_t)h->dims.nz; 
 
 DomainView view(ahx_handle* h) { return view_at(h, h->parity); }
 
+}  // namespace
+
+StepLaunch ahx::solo_launch(const ahx_handle* h, int parity) {
+  StepLaunch L;
+  L.precision = h->dims.precision;
+  L.mode = 0;
+  L.budget = false;
+  L.block_y = h->block_y;
+  L.zslab = h->zslab;
+  L.minb = h->minb;
+  L.pairs = h->pairs;
+  L.tma_ty = h->maps_ok ? h->tma_ty : 0;
+  L.tma_depth = h->tma_depth;
+  L.maps = L.tma_ty ? &h->maps[L.tma_ty == 8 ? 1 : 0][parity] : nullptr;
+  return L;
+}
+
+uint64_t ahx::solo_launch_key(const ahx_handle* h) {
+  const StepLaunch L = solo_launch(h, 0);
+  uint64_t k = 1469598103934665603ull;
+  const int v[] = {L.precision, L.block_y, L.zslab, L.minb, (int)L.pairs, L.tma_ty, L.tma_depth,
+                   h->jg0, h->nyg, h->jlo, h->jhi, h->dims.arith};
+  for (int x : v) k = (k ^ (uint64_t)(uint32_t)x) * 1099511628211ull;
+  return k | 1;   // never 0, the "no graph" key
+}
+
+cudaError_t ahx::solo_step(ahx_handle* h, int parity, cudaStream_t s) {
+  const StepLaunch L = solo_launch(h, parity);
+  const DomainView D = view_at(h, parity);
+  return h->dims.arith == AHX_ARITH_FAST ? fast::launch_step(D, L, s) : exact::launch_step(D, L, s);
+}
+
+namespace {
+
 using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                    const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
                                    CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
@@ -450,19 +484,11 @@ ahx_status ahx_set_parity(ahx_handle* h, int parity) {
   return AHX_OK;
 }
 
-// Everything a plain step's launches depend on besides the parity (buffers and tables are fixed per handle).
-static uint64_t launch_key(const ahx_handle* h, const StepLaunch& L) {
-  uint64_t k = 1469598103934665603ull;
-  const int v[] = {L.precision, L.block_y, L.zslab, L.minb, (int)L.pairs, L.tma_ty, L.tma_depth,
-                   h->jg0, h->nyg, h->jlo, h->jhi, h->dims.arith};
-  for (int x : v) k = (k ^ (uint64_t)(uint32_t)x) * 1099511628211ull;
-  return k | 1;   // never 0, the "no graph" key
-}
 
 // two plain steps starting at parity p, captured once per launch set-up and replayed (launch gaps matter for small
 // grids, where a step takes tens of microseconds)
 static ahx_status step_graph(ahx_handle* h, const StepLaunch& L0, int p, cudaGraphExec_t* out) {
-  const uint64_t key = launch_key(h, L0);
+  const uint64_t key = solo_launch_key(h);
   if (h->graph[p] && h->graph_key[p] == key) {
     *out = h->graph[p];
     return AHX_OK;
@@ -473,14 +499,7 @@ static ahx_status step_graph(ahx_handle* h, const StepLaunch& L0, int p, cudaGra
   cudaGraph_t g = nullptr;
   AHX_CUDA(h, cudaStreamBeginCapture(h->s_step, cudaStreamCaptureModeThreadLocal));
   cudaError_t e = cudaSuccess;
-  for (int s = 0; s < 2 && e == cudaSuccess; ++s) {
-    StepLaunch L = L0;
-    L.mode = 0;
-    const int par = p ^ s;
-    L.maps = L.tma_ty ? &h->maps[L.tma_ty == 8 ? 1 : 0][par] : nullptr;
-    const DomainView D = view_at(h, par);
-    e = h->dims.arith == AHX_ARITH_FAST ? fast::launch_step(D, L, h->s_step) : exact::launch_step(D, L, h->s_step);
-  }
+  for (int s = 0; s < 2 && e == cudaSuccess; ++s) e = solo_step(h, p ^ s, h->s_step);
   const cudaError_t e2 = cudaStreamEndCapture(h->s_step, &g);
   if (e != cudaSuccess || e2 != cudaSuccess) {
     if (g) cudaGraphDestroy(g);
@@ -499,15 +518,8 @@ static ahx_status step_graph(ahx_handle* h, const StepLaunch& L0, int p, cudaGra
 
 // the launch set-up of this handle's steps (mode and tensor maps are per step)
 static StepLaunch step_launch(const ahx_handle* h) {
-  StepLaunch L;
-  L.precision = h->dims.precision;
+  StepLaunch L = solo_launch(h, h->parity);
   L.budget = h->budget_on || h->accum_on;
-  L.block_y = h->block_y;
-  L.zslab = h->zslab;
-  L.minb = h->minb;
-  L.pairs = h->pairs;
-  L.tma_ty = h->maps_ok ? h->tma_ty : 0;
-  L.tma_depth = h->tma_depth;
   return L;
 }
 

@@ -65,6 +65,13 @@ struct ahx_batch {
   std::vector<cudaEvent_t> ev_member;
   cudaGraphExec_t graph[2] = {nullptr, nullptr};   // two steps starting at phase 0 / 1
   bool use_graph = true;
+  // branch mode: each member's own solo step kernels on parallel graph branches (side streams during capture)
+  bool branches = false;
+  std::vector<cudaStream_t> side;
+  std::vector<cudaEvent_t> side_ev;
+  cudaEvent_t fork_ev = nullptr;
+  cudaGraphExec_t bgraph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};   // [steps - 1][phase]
+  uint64_t bkey[2][2] = {{0, 0}, {0, 0}};
 };
 
 namespace {
@@ -124,6 +131,72 @@ int occupancy(const ahx_batch* b) {
 void drop_graphs(ahx_batch* b) {
   for (auto& g : b->graph)
     if (g) cudaGraphExecDestroy(g), g = nullptr;
+  for (auto& row : b->bgraph)
+    for (auto& g : row)
+      if (g) cudaGraphExecDestroy(g), g = nullptr;
+}
+
+constexpr int kMaxBranches = 32;   // concurrent branches of a branch-mode graph (members share them round-robin)
+
+// what a branch-mode graph depends on: the members, the parities they read at phase 0 and their launch shapes
+uint64_t branch_key(const ahx_batch* b) {
+  uint64_t k = 1469598103934665603ull;
+  for (size_t m = 0; m < b->members.size(); ++m) {
+    const ahx_handle* h = b->members[m];
+    for (uint64_t x : {(uint64_t)(uintptr_t)h, (uint64_t)b->base_parity[m], solo_launch_key(h)})
+      k = (k ^ x) * 1099511628211ull;
+  }
+  return k | 1;
+}
+
+// capture `nsteps` (1 or 2) steps starting at `phase` as one graph: member m's solo kernels, in step order, on branch
+// m mod K, the K branches forked from and joined back to the batch stream
+ahx_status capture_branches(ahx_batch* b, int phase, int nsteps) {
+  const size_t M = b->members.size();
+  const size_t K = std::min<size_t>(M, kMaxBranches);
+  if (!b->fork_ev) AHX_BCUDA(b, cudaEventCreateWithFlags(&b->fork_ev, cudaEventDisableTiming));
+  while (b->side.size() < K) {
+    cudaStream_t s = nullptr;
+    cudaEvent_t e = nullptr;
+    AHX_BCUDA(b, cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    b->side.push_back(s);
+    AHX_BCUDA(b, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    b->side_ev.push_back(e);
+  }
+  cudaGraphExec_t& slot = b->bgraph[nsteps - 1][phase];
+  if (slot) cudaGraphExecDestroy(slot), slot = nullptr;
+  cudaGraph_t g = nullptr;
+  AHX_BCUDA(b, cudaStreamBeginCapture(b->s, cudaStreamCaptureModeThreadLocal));
+  cudaError_t e = cudaEventRecord(b->fork_ev, b->s);
+  for (size_t k = 0; k < K && e == cudaSuccess; ++k) e = cudaStreamWaitEvent(b->side[k], b->fork_ev, 0);
+  for (size_t m = 0; m < M && e == cudaSuccess; ++m)
+    for (int s = 0; s < nsteps && e == cudaSuccess; ++s)
+      e = solo_step(b->members[m], b->base_parity[m] ^ phase ^ s, b->side[m % K]);
+  for (size_t k = 0; k < K && e == cudaSuccess; ++k) {
+    e = cudaEventRecord(b->side_ev[k], b->side[k]);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(b->s, b->side_ev[k], 0);
+  }
+  const cudaError_t e2 = cudaStreamEndCapture(b->s, &g);
+  if (e != cudaSuccess || e2 != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    return batch_fail(b, e != cudaSuccess ? e : e2, "batch branch graph capture");
+  }
+  const cudaError_t e3 = cudaGraphInstantiate(&slot, g, 0);
+  cudaGraphDestroy(g);
+  if (e3 != cudaSuccess) {
+    slot = nullptr;
+    return batch_fail(b, e3, "cudaGraphInstantiate");
+  }
+  b->bkey[nsteps - 1][phase] = branch_key(b);
+  return AHX_OK;
+}
+
+// the branch-mode graph of `nsteps` steps from the current phase, captured again when its key is stale
+ahx_status branch_graph(ahx_batch* b, int nsteps, cudaGraphExec_t* out) {
+  if (!b->bgraph[nsteps - 1][b->phase] || b->bkey[nsteps - 1][b->phase] != branch_key(b))
+    if (ahx_status st = capture_branches(b, b->phase, nsteps)) return st;
+  *out = b->bgraph[nsteps - 1][b->phase];
+  return AHX_OK;
 }
 
 ahx_status resize_grid(ahx_batch* b) {
@@ -317,6 +390,14 @@ void release(ahx_batch* b) {
   if (b->ev_done) cudaEventDestroy(b->ev_done);
   for (cudaEvent_t e : b->ev_member)
     if (e) cudaEventDestroy(e);
+  for (cudaStream_t s : b->side)
+    if (s) cudaStreamDestroy(s);
+  for (cudaEvent_t e : b->side_ev)
+    if (e) cudaEventDestroy(e);
+  if (b->fork_ev) cudaEventDestroy(b->fork_ev);
+  b->side.clear();
+  b->side_ev.clear();
+  b->fork_ev = nullptr;
   if (b->s) cudaStreamDestroy(b->s);
   b->ev_done = nullptr;
   b->ev_member.clear();
@@ -420,6 +501,7 @@ ahx_status ahx_batch_set_launch(ahx_batch* b, int minb, int zslab, int use_graph
   if (minb != 0 && minb != 4 && minb != 5 && minb != 6)
     return fail(AHX_EINVAL, "live solver: batch register-budget variant must be 4, 5 or 6 (0 = keep)");
   if (zslab < -1) return fail(AHX_EINVAL, "live solver: batch z-slab must be > 0, 0 (keep) or -1 (automatic)");
+  if (use_graph < 0 || use_graph > 2) return fail(AHX_EINVAL, "live solver: use_graph must be 0, 1 or 2");
   AHX_BCUDA(b, cudaSetDevice(b->dev));
   if (pairs > 0 && (b->arith != AHX_ARITH_FAST || b->precision == AHX_FP64))
     return fail(AHX_EINVAL, "live solver: paired levels need the FMA build and f32 arithmetic");
@@ -443,6 +525,7 @@ ahx_status ahx_batch_set_launch(ahx_batch* b, int minb, int zslab, int use_graph
     if (ahx_status st = install(b, b->members)) return st;
   }
   b->use_graph = use_graph != 0;
+  b->branches = use_graph == 2;
   return AHX_OK;
 }
 
@@ -472,6 +555,19 @@ ahx_status ahx_batch_step(ahx_batch* b, int n) {
     AHX_BCUDA(b, cudaStreamWaitEvent(b->s, b->ev_member[m], 0));
   }
   int left = n;
+  if (b->branches) {
+    cudaGraphExec_t g = nullptr;
+    if (left >= 2) {
+      if (ahx_status st = branch_graph(b, 2, &g)) return st;
+      for (; left >= 2; left -= 2) AHX_BCUDA(b, cudaGraphLaunch(g, b->s));
+    }
+    if (left == 1) {
+      if (ahx_status st = branch_graph(b, 1, &g)) return st;
+      AHX_BCUDA(b, cudaGraphLaunch(g, b->s));
+      b->phase ^= 1;
+      left = 0;
+    }
+  }
   if (b->use_graph) {
     if (!b->graph[b->phase])
       if (ahx_status st = capture(b, b->phase)) return st;
@@ -557,7 +653,7 @@ ahx_status ahx_batch_get_info(ahx_batch* b, ahx_batch_info_out* out) {
   out->tiles = b->ntiles;
   out->grid = b->grid;
   out->minb = b->minb;
-  out->use_graph = b->use_graph ? 1 : 0;
+  out->use_graph = b->branches ? 2 : (b->use_graph ? 1 : 0);
   out->pairs = b->pairs ? 1 : 0;
   out->zslab_max = b->zslab.empty() ? 0 : *std::max_element(b->zslab.begin(), b->zslab.end());
   out->cells = b->cells;

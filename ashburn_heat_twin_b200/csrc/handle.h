@@ -100,6 +100,9 @@ ahx_status fail(ahx_status st, const std::string& msg);                      // 
 ahx_status cuda_fail(ahx_handle* h, cudaError_t e, const char* what);       // marks h lost (if non-null)
 ahx_status check(ahx_handle* h);                                             // null / destroyed / lost
 DomainView view_at(ahx_handle* h, int parity);                               // the state read at this parity
+StepLaunch solo_launch(const ahx_handle* h, int parity);   // a plain step of this handle (its launch shape) at a parity
+uint64_t solo_launch_key(const ahx_handle* h);             // everything solo_launch depends on besides the parity
+cudaError_t solo_step(ahx_handle* h, int parity, cudaStream_t s);   // launch one plain step reading that parity
 ahx_status wait_event(ahx_handle* h, cudaEvent_t ev, int timeout_ms);        // bounded, lock not held
 
 }  // namespace ahx

@@ -427,8 +427,10 @@ class Batch:
         self._call('ahx_batch_sync', self.b, -1 if timeout_s is None else int(timeout_s * 1000))
 
     def set_launch(self, minb=0, zslab=0, use_graph=True, pairs=None):
-        self._call('ahx_batch_set_launch', self.b, int(minb), int(zslab), 1 if use_graph else 0,
-                   -1 if pairs is None else int(bool(pairs)))
+        """use_graph: True / 1 persistent launch replayed from a graph, False / 0 one persistent launch per step,
+        'branches' / 2 each member's own step kernel on parallel graph branches"""
+        g = 2 if use_graph in ('branches', 2) else (1 if use_graph else 0)
+        self._call('ahx_batch_set_launch', self.b, int(minb), int(zslab), g, -1 if pairs is None else int(bool(pairs)))
 
     def set_members(self, devices):
         self.devices = list(devices)

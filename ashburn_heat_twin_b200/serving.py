@@ -6,9 +6,10 @@ setNewCampuses, then step until a simulated time, then read()). The server runs 
 - admission: an arrived request takes a solver slot of its grid class (a recycled one, or a new one while the
   device-memory budget allows) as long as the resident cells stay under `max_cells`; otherwise it queues (FIFO);
 - a slot is configured exactly like a fresh page would be: setMet, setExistingFlux, setNewCampuses, resetFlow;
-- the active slots are stepped together by one LiveBatch (one persistent launch per step, CUDA-graph replay) in
-  chunks of at most `chunk` steps, never past any member's remaining steps; the member list follows the active
-  slots at chunk boundaries (continuous batching) through a stream-ordered table update;
+- the active slots are stepped together by one LiveBatch in chunks of at most `chunk` steps, never past any
+  member's remaining steps: by default each slot's own tuned step kernel on parallel branches of one CUDA graph per
+  two steps (the device runs the branches concurrently), or one persistent launch per step over all slots' tiles;
+  the member list follows the active slots at chunk boundaries (continuous batching);
 - chunks are queued ahead (up to `depth` in flight) so admission, set-up uploads and read-back overlap the device;
 - a finished request is answered with read() (surface theta, u, v and the u8 volume) and its slot returns to the
   pool of its class once that read has arrived.
@@ -61,25 +62,33 @@ def _state_bytes(solver):
         return solver.info['nCells'] * 52 * 4
 
 
-# launch of the serving batch on B200 (96-register variant, 8-level tiles): the fastest of the register variants x
-# tile depths on the 40/40/20 % mix of 40 / 30 / 20 m requests
-DEFAULT_BATCH_LAUNCH = dict(minb=5, zslab=8)
+# launch of the serving batch on B200: each request's own tuned step kernel on parallel graph branches, measured
+# 2-3 % above the best persistent launch (96-register variant, 8-level tiles) on the 40/40/20 % mix of 40 / 30 / 20 m
+# requests
+DEFAULT_BATCH_LAUNCH = dict(use_graph='branches')
 
 
 class Server:
     """Continuous-batching server on one device. `backend` builds a solver's device (CudaDevice by default);
     `batch_factory(solvers)` returns an object with step(n) -> Pending, set_members(solvers) and destroy()
     (LiveBatch by default); `batch_launch` holds its set_launch keywords (DEFAULT_BATCH_LAUNCH with LiveBatch, none
-    with another factory unless given)."""
+    with another factory unless given). `tune_slots` runs the launch-shape tuner on the first slot of each grid class
+    and gives later slots of the class the same shape, which the branch mode of the batch steps them with (default:
+    on in branch mode)."""
 
     def __init__(self, static, backend=None, batch_factory=None, max_cells=64_000_000, chunk=64, u10Max=8.0,
-                 hbm_budget_bytes=None, depth=2, clock=time.perf_counter, sleep=time.sleep, batch_launch=None):
+                 hbm_budget_bytes=None, depth=2, clock=time.perf_counter, sleep=time.sleep, batch_launch=None,
+                 tune_slots=None):
         self.static = static
+        self.class_launch: dict = {}
         self.backend = backend
         self.batch_factory = batch_factory or S.LiveBatch
         if batch_launch is None and batch_factory is None:
             batch_launch = DEFAULT_BATCH_LAUNCH
         self.batch_launch = dict(batch_launch) if batch_launch else None   # LiveBatch.set_launch keywords
+        if tune_slots is None:
+            tune_slots = bool(self.batch_launch) and self.batch_launch.get('use_graph') == 'branches'
+        self.tune_slots = bool(tune_slots)   # tune the first slot of each grid class, reuse its launch shape
         self.max_cells = int(max_cells)
         self.chunk = int(chunk)
         self.depth = max(1, int(depth))
@@ -101,8 +110,16 @@ class Server:
 
     # ---------------------------------------------------------------- slots
     def _new_solver(self, r: Request):
-        return S.create_live_solver(backend=self.backend, static=self.static, dx=r.dx, allowAnyDx=True,
-                                    heightM=r.heightM, u10Max=self.u10Max, met=r.met, existingFlux=r.flux)
+        s = S.create_live_solver(backend=self.backend, static=self.static, dx=r.dx, allowAnyDx=True,
+                                 heightM=r.heightM, u10Max=self.u10Max, met=r.met, existingFlux=r.flux)
+        if self.tune_slots:
+            key = (r.dx, r.heightM)
+            if key not in self.class_launch:
+                by, zs, _ = s._dev.autotune(3)          # trials run on a scratch copy of the state
+                self.class_launch[key] = (by, zs)
+            else:
+                s._dev.set_launch(*self.class_launch[key])
+        return s
 
     def _take_slot(self, r: Request):
         key = (r.dx, r.heightM)

@@ -554,12 +554,15 @@ class LiveBatch:
 
     def set_launch(self, minb=0, zslab=0, use_graph=True, pairs=None):
         """register-budget variant (4 / 5 / 6, 0 = keep), tile depth (levels, 0 = keep, -1 = whole columns), graph
-        replay on or off, paired levels on packed f32x2 arithmetic (None = keep)."""
+        replay on or off, paired levels on packed f32x2 arithmetic (None = keep). use_graph='branches' steps each
+        member with its own solo kernel and launch shape on parallel branches of one graph instead of the persistent
+        launch."""
         self._b.set_launch(minb, zslab, use_graph, pairs)
 
     def autotune(self, steps_per_trial=4):
         """time the register-budget variants x tile depths on the batch itself and keep the fastest. Like
-        benchmark(), the trials advance every member's state (by up to 24 x (2 + steps_per_trial) steps)."""
+        benchmark(), the trials advance every member's state (by up to 25 x (2 + steps_per_trial) steps). The last
+        candidate is the branch mode (each member's own launch shape, so tune the members first)."""
         paired = (False, True) if self.solvers[0]._dev.arith == 'fast' and self.solvers[0]._dev.precision != 'fp64' \
             else (False,)
         best = None
@@ -572,8 +575,15 @@ class LiveBatch:
                     self._advance(2 + steps_per_trial)
                     if best is None or ms < best[0]:
                         best = (ms, minb, zs, pr)
+        # each member's own tuned kernel on parallel graph branches
+        self._b.set_launch(0, 0, 'branches', None)
+        self._b.time_steps(2)
+        ms = self._b.time_steps(steps_per_trial)
+        self._advance(2 + steps_per_trial)
+        if ms < best[0]:
+            return dict(mode='branches', ms_per_step=ms / steps_per_trial)
         self._b.set_launch(best[1], best[2], True, best[3])
-        return dict(minb=best[1], zslab=best[2], pairs=best[3], ms_per_step=best[0] / steps_per_trial)
+        return dict(mode='persistent', minb=best[1], zslab=best[2], pairs=best[3], ms_per_step=best[0] / steps_per_trial)
 
     def destroy(self):
         """release the batch (idempotent); the members stay alive."""

@@ -324,8 +324,9 @@ def main_batch(a, rank, world, local, dist, torch):
 
 
 def main_serve(a, rank, world, local, dist, torch):
-    """The serving workload: a seeded Poisson trace of requests served with continuous batching (one persistent
-    launch per step over all admitted requests, chunks of --chunk steps, admission under a cell budget). Reports the
+    """The serving workload: a seeded Poisson trace of requests served with continuous batching (the admitted
+    requests' own tuned step kernels on parallel branches of one graph per two steps, or with --batch-mode persistent
+    one persistent launch per step over all of them; chunks of --chunk steps, admission under a cell budget). Reports the
     aggregate served rate, latency percentiles and queueing delay, and the same trace solved back to back (FIFO, each
     request alone at its class's measured solo rate)."""
     import numpy as np
@@ -343,7 +344,10 @@ def main_serve(a, rank, world, local, dist, torch):
     # through the same server (kernels, graph capture, read-back staging)
     # admission by free device memory (80 % of what is free now) as well as by the resident-cell budget
     free_b, _ = torch.cuda.mem_get_info(local)
-    blaunch = dict(minb=a.batch_minb, zslab=a.batch_zslab) if (a.batch_minb or a.batch_zslab) else None
+    if a.batch_minb or a.batch_zslab or a.batch_mode == 'persistent':
+        blaunch = dict(minb=a.batch_minb or 5, zslab=a.batch_zslab or 8)
+    else:
+        blaunch = dict(use_graph='branches')
     srv = SV.Server(st, backend=backend, max_cells=a.max_cells, chunk=a.chunk, hbm_budget_bytes=int(0.8 * free_b),
                     batch_launch=blaunch)
     per_req = sum(sh * (6000 // dx) ** 2 * round(hm / dx) for sh, dx, hm in SC.SERVE_MIX)
@@ -576,6 +580,9 @@ def main():
     ap.add_argument('--chunk', type=int, default=64, help='serving: steps per batched chunk')
     ap.add_argument('--batch-minb', type=int, default=0, help='serving: batch register variant (4 / 5 / 6; 0 = default)')
     ap.add_argument('--batch-zslab', type=int, default=0, help='serving: batch tile depth in levels (0 = default)')
+    ap.add_argument('--batch-mode', default='branches', choices=['persistent', 'branches'],
+                    help='serving: one persistent launch over tiles, or each request\'s own tuned kernel on parallel '
+                         'graph branches')
     ap.add_argument('--spin-s', type=float, default=120.0, help='precision study: simulated spin-up seconds')
     ap.add_argument('--mean-s', type=float, default=600.0, help='precision study: simulated averaging seconds')
     ap.add_argument('--kicks', type=float, nargs='*', default=None,

@@ -272,8 +272,10 @@ ahx_status ahx_batch_time_steps(ahx_batch* b, int n, int timeout_ms, float* ms);
 ahx_status ahx_batch_sync(ahx_batch* b, int timeout_ms);
 /* launch set-up: register-budget variant 4 / 5 / 6 (0 = keep); tile depth zslab in levels for every member (clipped
  * to its nz; 0 = keep; -1 = whole columns when that leaves at least 4 tiles per persistent block, else each member's
- * own z-slab); whether steps replay the captured graph (1) or launch one kernel per step (0); paired levels on packed
- * f32x2 arithmetic (1 on, 0 off, -1 keep; FMA build, f32 arithmetic only) */
+ * own z-slab); use_graph: 1 = steps replay the captured graph of the persistent launch, 0 = one persistent launch per
+ * step, 2 = steps replay a graph of each member's own solo step kernel (its own launch shape, e.g. from
+ * ahx_autotune) on parallel branches, which the device runs concurrently (minb, zslab and pairs then do not apply);
+ * paired levels on packed f32x2 arithmetic (1 on, 0 off, -1 keep; FMA build, f32 arithmetic only) */
 ahx_status ahx_batch_set_launch(ahx_batch* b, int minb, int zslab, int use_graph, int pairs);
 ahx_status ahx_batch_get_info(ahx_batch* b, ahx_batch_info_out* out);
 ahx_status ahx_batch_destroy(ahx_batch* b);   /* idempotent; members are released */

@@ -154,3 +154,35 @@ def test_batch_paired_levels_match_solo():
     b.destroy()
     for s in solo + mem:
         s.destroy()
+
+
+@pytest.mark.parametrize('precision', ['fp32', 'fp16sr'])
+def test_batch_branches_match_solo(precision):
+    """Branch mode: each member's own solo kernel (its own launch shape) on parallel graph branches, with odd step
+    counts (a one-step graph), membership changes and solo steps in between, leaves every member bit-identical to
+    stepping it alone."""
+    solo = [scenario(i, precision, 'fast') for i in range(3)]
+    mem = [scenario(i, precision, 'fast') for i in range(3)]
+    for a, m, shape in zip(solo, mem, ((2504, 3), (604, 2), (404, 0))):
+        for s in (a, m):
+            s._dev.set_launch(*shape)
+    b = LiveBatch(mem)
+    b.set_launch(use_graph='branches')
+    assert b.info['use_graph'] == 2
+    b.step(7).result()
+    for s in solo:
+        s.step(7).result()
+    for a, m in zip(solo, mem):
+        same(a, m)
+    mem[1].step(3).result()
+    solo[1].step(3).result()
+    b.set_members([mem[2], mem[1]])
+    b.step(4).result()
+    for s in (solo[2], solo[1]):
+        s.step(4).result()
+    for a, m in zip(solo, mem):
+        same(a, m)
+    b.destroy()
+    for s in solo + mem:
+        s.destroy()
+
