@@ -609,6 +609,39 @@ __device__ __forceinline__ void fast_pair(const DomainView& D, const ParamsHead&
       });
 }
 
+// Population slot p of a cell update: f population p (p < 19) or g population p - 19 (p < 26). Bit p of these masks
+// is set where the slot's velocity has that y / z component (+1 or -1).
+constexpr uint32_t slot_mask(int comp, int sign) {
+  uint32_t m = 0;
+  for (int p = 0; p < 26; ++p) {
+    const int c = p < 19 ? kC19[p][comp] : kC7[p - 19][comp];
+    if (c == sign) m |= 1u << p;
+  }
+  return m;
+}
+
+// L2 prefetch of the interior pull sources of level k for the warp's 32 columns (row base: the first column's cell
+// index in its plane): lane p < 26 touches the 128-byte line of slot p's source row, x-aligned to the warp (the one
+// element a +-x shift moves across the line edge is left to the load). The offsets are clamped into the population
+// buffers, so edge rows and levels never reach outside them. No state is read or written: a hint that puts the
+// next level's rows in flight while this one is relaxed.
+template <class S>
+__device__ __forceinline__ void prefetch_level(const DomainView& D, int k, uint32_t rowbase) {
+  const int lane = threadIdx.x & 31;
+  if (lane >= 26) return;
+  constexpr uint32_t kYp = slot_mask(1, 1), kYn = slot_mask(1, -1), kZp = slot_mask(2, 1), kZn = slot_mask(2, -1);
+  const int cy = (int)((kYp >> lane) & 1u) - (int)((kYn >> lane) & 1u);
+  const int cz = (int)((kZp >> lane) & 1u) - (int)((kZn >> lane) & 1u);
+  const bool isf = lane < 19;
+  const int q = isf ? lane : lane - 19;
+  const int64_t n = (int64_t)q * D.qs + (int64_t)(k - cz) * D.ps + (int64_t)rowbase - (int64_t)cy * D.px;
+  const int64_t lim = (int64_t)(isf ? 19 : 7) * D.qs - 64;
+  const int64_t e = n < 0 ? 0 : (n > lim ? lim : n);
+  const char* p = isf ? static_cast<const char*>(D.fA) + e * (int64_t)sizeof(StoreF<S>)
+                      : static_cast<const char*>(D.gA) + e * (int64_t)sizeof(StoreG<S>);
+  asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+
 // Budget accumulators of one thread (summed over its cells, then reduced per block into FP64).
 struct BudgetAcc {
   float theta, src, cells;
@@ -675,8 +708,18 @@ __device__ __forceinline__ void step_block(const DomainView& D, int bx, int by, 
   // PAIRS (FMA build without output modes): two interior levels at a time on the packed f32x2 lanes when every
   // active lane of the warp has both cells interior (bit-identical to the single-level path; more registers)
   constexpr bool kPairs = PAIRS && FAST && MODE == 0 && !BUDGET && std::is_same_v<R, float>;
+  // FMA build, plain steps, launch option: the next level's (pair's) source rows are prefetched into L2 one level
+  // (pair) ahead
+  constexpr bool kPrefetch = FAST && MODE == 0 && !BUDGET;
+  const uint32_t rowbase = (uint32_t)j * (uint32_t)D.px + (uint32_t)(bx * kBlockX);
 #pragma unroll 1
   for (int k = kw; k < k1; ++k) {
+    if constexpr (kPrefetch) {
+      if (D.pf) {
+        if (k + (kPairs ? 2 : 1) < k1) prefetch_level<S>(D, k + (kPairs ? 2 : 1), rowbase);
+        if (kPairs && k + 3 < k1) prefetch_level<S>(D, k + 3, rowbase);
+      }
+    }
     if constexpr (kPairs) {
       if (k + 1 < k1) {
         const bool in2 = valid && k >= C.kg && !C.face && k >= C.kint && k + 1 < D.nz - 1;

@@ -80,6 +80,7 @@ struct ahx_handle {
   bool maps_ok = false;
   ahx::TmaMaps maps[2][2];                     // [TY 4 / 8][parity]: tensor maps of the state read by a step
   int* d_err = nullptr;                   // error word the staged kernel sets
+  bool prefetch = false;                  // next-level L2 prefetch in the step (launch option, FMA build)
   uint32_t* d_tick = nullptr;             // step counter pair of the stochastic-rounding storage, then the tuner's
   ahx::ReadSlot reads[AHX_MAX_READS];
   uint64_t next_read = 0;

@@ -269,6 +269,7 @@ struct DomainView {
   // the last block of a step to finish advances [0]. tick_blocks: blocks (tiles) of one step in a batched launch
   uint32_t* tick;
   uint32_t tick_blocks;
+  int pf;                       // 1: the FMA build's plain step prefetches the next level's source rows into L2
   int nx, ny, nz, px;
   // y-slab of a larger domain: local row 0 is global row jg0 of nyg; only local rows [jlo, jhi) are updated (the
   // others are ghost rows refreshed from the neighbouring slabs); a whole domain has jg0 0, nyg ny, [0, ny)

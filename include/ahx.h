@@ -203,8 +203,9 @@ ahx_status ahx_accum_read(ahx_handle* h, double* surf3, double* faces, int64_t* 
 /* launch shape of the fused step: block_y = threads per block in y (x is one warp) plus 100 x the register-budget
  * variant (0: compiler's choice; 4, 5 or 6: 128-thread blocks, that many resident per SM, only with block_y 4), plus
  * 2000 for paired levels (two interior levels per thread on packed f32x2 arithmetic; FMA build, f32 arithmetic; the
- * results are bit-identical to unpaired); or, for the TMA-staged kernel, 1000 + 100 x stages + rows (rows 4 with
- * 2-4 stages, rows 8 with 2-3 stages); zslab = z-slab depth in levels; 0 = keep */
+ * results are bit-identical to unpaired), plus 10000 for an L2 prefetch of the next level's source rows (FMA build;
+ * a hint that changes no result); or, for the TMA-staged kernel, 1000 + 100 x stages + rows (rows 4 with 2-4 stages,
+ * rows 8 with 2-3 stages); zslab = z-slab depth in levels; 0 = keep */
 ahx_status ahx_set_launch(ahx_handle* h, int block_y, int zslab);
 /* time candidate launch shapes on scratch copies of the state and keep the fastest; the state is not advanced;
  * *best_block_y uses the encoding of ahx_set_launch */

@@ -189,7 +189,8 @@ def test_budget_record_matches_step_outputs():
 def test_autotune_keeps_state():
     g, o = _pair()
     by, zs, ms = g._dev.autotune(2)
-    plain = by - 2000 if by >= 2000 else by          # 2000 + ...: paired levels (FMA build only)
+    plain = by % 10000                                # 10000 + ...: L2 prefetch (FMA build only)
+    plain = plain - 2000 if plain >= 2000 else plain  # 2000 + ...: paired levels (FMA build only)
     assert plain % 100 in (2, 4, 8) and plain // 100 in (0, 4, 5, 6) and zs >= 1 and ms > 0
     for s in (g, o):
         s.step(4).result()
@@ -217,14 +218,14 @@ def test_launch_shapes_bit_exact(shape, zslab):
 @pytest.mark.parametrize('precision', ['fp32', 'fp16', 'fp16g32', 'fp16sr'])
 def test_paired_levels_bit_identical(precision):
     """The FMA build's paired path (two interior levels per thread on packed f32x2 arithmetic, launch shapes
-    2404 / 2504 / 2604) leaves exactly the state and outputs of the unpaired path, with whole columns and with odd
-    z-slabs (which change how levels pair)."""
+    2404 / 2504 / 2604) and the L2-prefetch option (10000 +) leave exactly the state and outputs of the unpaired
+    path, with whole columns and with odd z-slabs (which change how levels pair)."""
     met = dict(u10=5.0, dirFrom=300.0, wstar=1.5, blh=700.0)
     ref = small_solver(cuda_backend(precision, 'fast'), met=met)
     ref._dev.set_launch(404, 0)
     ref.step(9).result()
     fr, gr = ref._dev.read_state()
-    for shape, zs in ((2404, 0), (2504, 7), (2604, 5)):
+    for shape, zs in ((2404, 0), (2504, 7), (2604, 5), (12504, 3), (10404, 4)):
         s = small_solver(cuda_backend(precision, 'fast'), met=met)
         s._dev.set_launch(shape, zs)
         s.step(9).result()
