@@ -32,7 +32,7 @@ class SynthSpec:
     seed: int = 1
 
 
-# BASELINE configurations (the reference publishes no synthetic inputs; these are our seeded stand-ins)
+# Benchmark configurations (the reference publishes no synthetic inputs; these are our seeded stand-ins)
 C1 = SynthSpec(hills=8, relief_m=30.0, buildings=1500, side_m=(20.0, 120.0), height_m=(8.0, 30.0), dc_count=60,
                seed=1)
 C2 = SynthSpec(hills=24, relief_m=40.0, buildings=4000, side_m=(15.0, 150.0), height_m=(8.0, 40.0), dc_count=211,
