@@ -576,7 +576,8 @@ def main():
     ap.add_argument('--requests', type=int, default=48, help='serving: requests in the trace')
     ap.add_argument('--rate', type=float, default=50.0, help='serving: mean arrival rate (requests/s)')
     ap.add_argument('--seed', type=int, default=5, help='serving: trace seed')
-    ap.add_argument('--max-cells', type=int, default=64_000_000, help='serving: resident cell budget')
+    ap.add_argument('--max-cells', type=int, default=24_000_000,
+                    help='serving: resident cell budget (24 M: the served rate of 64 M at a lower p50)')
     ap.add_argument('--chunk', type=int, default=64, help='serving: steps per batched chunk')
     ap.add_argument('--batch-minb', type=int, default=0, help='serving: batch register variant (4 / 5 / 6; 0 = default)')
     ap.add_argument('--batch-zslab', type=int, default=0, help='serving: batch tile depth in levels (0 = default)')
