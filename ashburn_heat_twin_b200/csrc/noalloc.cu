@@ -1,9 +1,8 @@
 // Diagnostics over a caller-owned state with no allocation of any kind: ahx_stats_noalloc (include/ahx.h).
 //
-// Who needs this: callers that cannot allocate device memory at the moment they want diagnostics, such as a host
-// that records its work into a CUDA graph (cudaMalloc is not allowed during stream capture), an engine that has
-// handed all device memory to a fixed pool up front, or code running where a driver call that may allocate would
-// block. They still own the state (populations f, g and the ktop plane, in device memory, reference layout) and an
+// Who needs this: callers that cannot allocate device memory at the moment they want diagnostics, such as an engine
+// that has handed all device memory to a fixed pool up front (an allocation outside the pool can fail or break its
+// budget), or code on a latency-critical path where cudaMalloc / cudaFree would synchronise the device. They still own the state (populations f, g and the ktop plane, in device memory, reference layout) and an
 // output record in device memory; this entry point only launches kernels on the caller's stream.
 //
 // The reduction's per-block partial sums live in one file-scope device array, g_stats_partials, of a fixed size

@@ -1,5 +1,5 @@
-"""ahx_stats_noalloc: diagnostics for callers that cannot allocate device memory when they ask for them (a host
-recording a CUDA graph, an engine whose memory all belongs to its own pool). The caller owns every buffer; the entry
+"""ahx_stats_noalloc: diagnostics for callers that cannot allocate device memory when they ask for them (an engine
+whose device memory all belongs to its own pool, or a latency-critical path where an allocation would synchronise). The caller owns every buffer; the entry
 point keeps its per-block partial sums in a fixed scratch array inside the library.
 
 Checked through the C ABI against ahx_stats on the same state, on two calls in a row, with the tolerance the other
