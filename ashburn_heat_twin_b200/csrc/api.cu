@@ -1034,16 +1034,9 @@ ahx_status ahx_autotune(ahx_handle* h, int steps_per_trial, int* best_block_y, i
                                {4, 4, 0, 0, false}, {4, 5, 0, 0, false}, {4, 6, 0, 0, false}};
   if (h->dims.arith == AHX_ARITH_FAST && h->dims.precision != AHX_FP64)
     for (Shape sh : {Shape{4, 4, 0, 0, true}, Shape{4, 5, 0, 0, true}, Shape{4, 6, 0, 0, true}}) shapes.push_back(sh);
-  // staged (TMA) shapes, with tensor maps over the scratch copies the trials step
-  TmaMaps tm[2][2];
-  bool tma_ok = h->maps_ok;
-  for (int t = 0; t < 2 && tma_ok; ++t) {
-    tma_ok = make_maps(h, f0, g0, t ? 8 : 4, &tm[t][0]) && make_maps(h, f1, g1, t ? 8 : 4, &tm[t][1]);
-  }
-  if (tma_ok)
-    for (Shape sh : {Shape{4, 0, 4, 2, false}, Shape{4, 0, 4, 3, false}, Shape{4, 0, 4, 4, false},
-                     Shape{8, 0, 8, 2, false}, Shape{8, 0, 8, 3, false}})
-      shapes.push_back(sh);
+  // The TMA-staged kernel is not a candidate: it never won a trial (16-20 against 26.6 GLUPS on 600x600x64) and an
+  // early build of it once stopped with a misaligned-address error whose cause was not found. It stays reachable only
+  // through an explicit ahx_set_launch value.
   // thin slabs put more blocks in flight on small grids, where one 6-level wave leaves the SMs latency-bound
   std::vector<int> zss = {h->dims.nz, 32, 16, 12, 8, 6, 4, 3, 2};
   DomainView D = view(h);
@@ -1072,7 +1065,7 @@ ahx_status ahx_autotune(ahx_handle* h, int steps_per_trial, int* best_block_y, i
         D.gA = (s & 1) ? g1 : g0;
         D.gB = (s & 1) ? g0 : g1;
         set_pointers(D, h->esize, h->esize_g);
-        L.maps = sh.ty ? &tm[sh.ty == 8 ? 1 : 0][s & 1] : nullptr;
+        L.maps = nullptr;
         const cudaError_t e = h->dims.arith == AHX_ARITH_FAST ? fast::launch_step(D, L, h->s_step)
                                                                 : exact::launch_step(D, L, h->s_step);
         if (e != cudaSuccess) return cuda_fail(h, e, "autotune launch");

@@ -10,6 +10,7 @@
 // exits. Every call on a device shares it and it keeps the last call's contents; each call overwrites every slot it
 // later reads, so nothing has to start at zero. Two calls whose kernels overlap on the GPU (different streams without
 // ordering between them) race on the array: order them, or use ahx_stats on a handle.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstring>
@@ -44,10 +45,40 @@ ahx_status fail(ahx_status st, const std::string& m) {
   return st;
 }
 
-// per-device address of g_stats_partials, looked up once per device with that device current
+// Per-device address of g_stats_partials, looked up once per device (with that device current) and again whenever
+// the device's current context is a different one than at the look-up (after cudaDeviceReset, or a context the
+// caller made itself): an address belongs to the context it was resolved in.
 constexpr int kMaxDevices = 64;
 std::mutex g_mu;
 Partial* g_addr[kMaxDevices] = {nullptr};
+unsigned long long g_ctx[kMaxDevices] = {0};
+
+// unique id of the calling thread's current context (driver entry points found through the runtime, so the library
+// needs no link to the driver library); 0 when there is no current context or the driver cannot say
+unsigned long long current_context_id() {
+  using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+  using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long*);
+  static CtxGetCurrentFn get_current = nullptr;
+  static CtxGetIdFn get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = reinterpret_cast<CtxGetCurrentFn>(p);
+    p = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<CtxGetIdFn>(p);
+    cudaGetLastError();
+  });
+  CUcontext c = nullptr;
+  unsigned long long id = 0;
+  if (!get_current || !get_id || get_current(&c) != CUDA_SUCCESS || c == nullptr || get_id(c, &id) != CUDA_SUCCESS)
+    return 0;
+  return id;
+}
 
 // Block b reduces cells [b*kCellsPerBlock, (b+1)*kCellsPerBlock) of the reference layout (cell = (k*ny + j)*nx + i)
 // in a fixed order and writes its partial record; the same per-cell f32 values as the stats kernel (kernel.js:580-633).
@@ -190,15 +221,19 @@ extern "C" ahx_status ahx_stats_noalloc(int nx, int ny, int nz, const float* f, 
     return fail(AHX_EDEVICE, "live solver: ahx_stats_noalloc: no usable current CUDA device");
   Partial* parts = nullptr;
   {
-    // set-up, once per device, with that device current: the device address of the scratch array
+    // set-up, once per device and context, with that device current: the device address of the scratch array
     std::lock_guard<std::mutex> lk(g_mu);
-    if (!g_addr[dev]) {
+    const unsigned long long ctx = current_context_id();
+    if (!g_addr[dev] || ctx == 0 || ctx != g_ctx[dev]) {
       void* p = nullptr;
       const cudaError_t e = cudaGetSymbolAddress(&p, g_stats_partials);
-      if (e != cudaSuccess || !p)
+      if (e != cudaSuccess || !p) {
+        g_addr[dev] = nullptr;
         return fail(AHX_EDEVICE, std::string("live solver: ahx_stats_noalloc: cannot resolve its scratch (") +
                                      cudaGetErrorString(e) + ")");
+      }
       g_addr[dev] = static_cast<Partial*>(p);
+      g_ctx[dev] = current_context_id();   // the look-up made the device's primary context current if none was
     }
     parts = g_addr[dev];
   }

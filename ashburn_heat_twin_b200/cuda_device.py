@@ -340,6 +340,12 @@ class CudaDevice:
 
     def set_launch(self, block_y=0, zslab=0):
         self._c('ahx_set_launch', int(block_y), int(zslab))
+        prev = getattr(self, '_launch', (0, 0))
+        self._launch = (int(block_y) or prev[0], int(zslab) or prev[1])
+
+    def launch(self):
+        """(block_y, zslab) in the ahx_set_launch encoding as last set or tuned; (0, 0) = the library's default."""
+        return getattr(self, '_launch', (0, 0))
 
     def set_slab(self, jg0, nyg, jlo, jhi):
         self._c('ahx_set_slab', int(jg0), int(nyg), int(jlo), int(jhi))
@@ -377,6 +383,7 @@ class CudaDevice:
     def autotune(self, steps_per_trial=4):
         by, zs, ms = ctypes.c_int(), ctypes.c_int(), ctypes.c_float()
         self._c('ahx_autotune', int(steps_per_trial), ctypes.byref(by), ctypes.byref(zs), ctypes.byref(ms))
+        self._launch = (by.value, zs.value)
         return by.value, zs.value, ms.value
 
     def info(self):

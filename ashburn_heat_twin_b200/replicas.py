@@ -36,3 +36,18 @@ def barrier(dist=None, sync=None):
 def aggregate_rate(units_per_rank, world, seconds_max):
     """Whole-job throughput of weak-scaled replicas: every rank processed units_per_rank in at most seconds_max."""
     return world * units_per_rank / seconds_max
+
+
+def launch_ranks(script, argv, n, port=None):
+    """Run `script argv` as n ranks on this node under torch.distributed.run (rendezvous on 127.0.0.1) and return the
+    launcher's exit status; every rank reads RANK / LOCAL_RANK / WORLD_SIZE from its environment."""
+    import socket
+    import subprocess
+    import sys
+    if port is None:
+        with socket.socket() as sk:
+            sk.bind(('127.0.0.1', 0))
+            port = sk.getsockname()[1]
+    cmd = [sys.executable, '-m', 'torch.distributed.run', '--nnodes=1', f'--nproc-per-node={int(n)}',
+           '--master-addr', '127.0.0.1', '--master-port', str(port), script] + list(argv)
+    return subprocess.call(cmd)

@@ -11,9 +11,11 @@ is far larger than L2, so no flush is needed between steps. `e2e` runs the same 
 (create_live_solver / setMet / step / read) with host buffers: every frame uploads a parameter block from host
 memory, advances F steps and reads back the near-surface fields and the u8 volume, as the live app does.
 
---gpus N runs N independent replicas, one per rank (the path does not shard: "replicas only", weak scaling).
+--gpus N runs N independent replicas, one per rank (the path does not shard: "replicas only", weak scaling). Under
+torchrun the ranks come from the environment; without it, --gpus N > 1 starts N ranks itself (torch.distributed.run
+on 127.0.0.1, one process per GPU) and returns their exit status.
 --impl reference times the CPU restatement of the reference kernels (the reference itself is WebGPU/WGSL and cannot
-run here) on all host cores, rank 0 only.
+run here) on all host cores, rank 0 only; its line reports n_gpus 0 (no GPU takes part).
 """
 from __future__ import annotations
 
@@ -102,13 +104,22 @@ def measured_peaks():
         return 6650.0, 'fallback'
 
 
-def profile_traffic(precision):
-    """DRAM bytes per launch of the step kernel from the committed ncu summary, scaled to the 600x600x64 launch."""
+def profile_traffic(precision, launch, fluid):
+    """DRAM bytes per launch of the step kernel from the committed ncu summary of the same storage, arithmetic and
+    launch shape (profiles/step_<precision>_traffic.json), scaled by fluid cells to this launch. Returns (bytes,
+    source note); bytes is None when no capture of this launch shape exists."""
     p = os.path.join(ROOT, 'profiles', f'step_{precision}_traffic.json')
     try:
-        return json.load(open(p))['dram_bytes_per_launch_scaled']
+        d = json.load(open(p))
     except Exception:
-        return None
+        return None, 'no ncu capture committed for this storage'
+    got = (d.get('block_y'), d.get('zslab'))
+    if launch is None or tuple(launch) != got:
+        return None, (f'the committed capture is of launch {got[0]} / zslab {got[1]}, not the timed launch '
+                      f'{launch[0] if launch else None} / zslab {launch[1] if launch else None}')
+    return d['dram_bytes_per_fluid_cell'] * fluid, (
+        f"ncu dram__bytes_read.sum + dram__bytes_write.sum of the same launch shape on {d['grid']} "
+        f"({d['dram_bytes_per_fluid_cell']:.1f} B per fluid cell), scaled by fluid cells")
 
 
 class Clocks:
@@ -158,10 +169,19 @@ class Clocks:
                     if any(r[3].strip().replace('.', '', 1).isdigit() for r in rows) else None)
 
 
+def host_threads():
+    """Host threads this process may run on."""
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
 def cpu_baseline(seconds=10.0, max_steps=30, workload='c2'):
     """The oracle (CPU restatement of the reference kernels) on full steps of the workload, all host threads."""
     import numpy as np
     from oracle import oracle as O
+    O.set_threads(host_threads())
     s = make_solver(backend=lambda nx, ny, nz: O.OracleDevice(nx, ny, nz), workload=workload)
     threads = O.max_threads()
     dev = s._dev
@@ -179,11 +199,19 @@ def cpu_baseline(seconds=10.0, max_steps=30, workload='c2'):
                        f'({cells * n / 1e6:.0f} M cell updates, {t:.1f} s)')
 
 
+def bench_config(workload, precision, cells):
+    """The config dict both arms print for a workload (identical keys and values for the same workload)."""
+    return dict(workload=WORKLOADS[workload]['desc'], precision=precision, scheme='pull', parallelism='replicas',
+                l2=f'inputs larger than L2, no flush: state {2 * 26 * cells * CELL_BYTES[precision] / 208 / 1e9:.2f} '
+                   f'GB per replica against a 126 MB L2')
+
+
 def run_reference(a, rank):
     if rank != 0:
         return 0
     import numpy as np
     from oracle import oracle as O
+    O.set_threads(host_threads())   # every host thread, also under torchrun (which sets OMP_NUM_THREADS=1)
     s = make_solver(backend=lambda nx, ny, nz: O.OracleDevice(nx, ny, nz))
     dev = s._dev
     dev.step(a.warmup, 0)
@@ -192,10 +220,11 @@ def run_reference(a, rank):
     t = time.perf_counter() - t0
     cells = s.info['nCells']
     v = cells * a.steps / t / 1e9
-    out = dict(metric=METRIC, value=v, unit='GLUPS', n_gpus=a.gpus, steps=a.steps, warmup=a.warmup,
+    out = dict(metric=METRIC, value=v, unit='GLUPS', n_gpus=0, steps=a.steps, warmup=a.warmup,
                ms_per_step=t / a.steps * 1e3, higher_is_better=True, scaling='weak', vs_baseline=None, dtype='f32',
-               data='synthetic', impl='reference',
-               config=dict(workload=WORKLOADS['c2']['desc'], precision='fp32', scheme='pull', parallelism='replicas'),
+               data='synthetic (seeded terrain and buildings; no public dataset involved)', impl='reference',
+               devices=f'host CPU only ({O.max_threads()} threads, rank 0); no GPU takes part',
+               config=bench_config('c2', 'fp32', cells),
                cpu_baseline=dict(value=v, unit='GLUPS', cores=O.max_threads(), kind='port',
                                  sample=f'{a.steps} full steps after {a.warmup} warm-up steps'),
                e2e=dict(value=v, unit='GLUPS', h2d_bytes_per_step=0, d2h_bytes_per_step=0))
@@ -555,6 +584,34 @@ def main_precision(a, rank, world, local, dist, torch):
     return 0
 
 
+def ranks_check(a, rank, world, local):
+    """The multi-rank plumbing of the benchmark without the stepping: process group (NCCL on GPUs, gloo without
+    CUDA), the barrier around the timed region and the max-over-ranks reduction. Rank 0 prints one JSON line."""
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+    cuda = torch.cuda.is_available()
+    if world > 1:
+        if cuda:
+            torch.cuda.set_device(local)
+            dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=60),
+                                    device_id=torch.device('cuda', local))
+        else:
+            dist.init_process_group('gloo', timeout=datetime.timedelta(seconds=60))
+    pg = dist if world > 1 else None
+    RP.barrier(pg)
+    top = RP.max_over_ranks(rank, pg, f'cuda:{local}' if cuda else 'cpu')
+    out = dict(n_gpus=world if cuda else 0, ranks=world, max_rank_seen=int(top), backend=(
+        'nccl' if cuda else 'gloo') if world > 1 else None)
+    if pg is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
@@ -588,12 +645,22 @@ def main():
     ap.add_argument('--mean-s', type=float, default=600.0, help='precision study: simulated averaging seconds')
     ap.add_argument('--kicks', type=float, nargs='*', default=None,
                     help='precision study: also run FP64 with one relative kick of each size after the spin-up')
+    ap.add_argument('--ranks-check', action='store_true',
+                    help='start the ranks, run the barrier and the max-over-ranks reduction, print the rank count and '
+                         'exit (no stepping; gloo when CUDA is unavailable)')
     a = ap.parse_args()
     a.warmup = max(a.warmup, 3)
 
     rank, world, local = RP.env_ranks()
     if a.impl == 'reference':
         return run_reference(a, rank)
+    if a.gpus > 1 and 'WORLD_SIZE' not in os.environ:
+        return RP.launch_ranks(os.path.abspath(__file__), sys.argv[1:], a.gpus)
+    if 'WORLD_SIZE' in os.environ and world != a.gpus:
+        log(f'bench.py: --gpus {a.gpus} but the launcher started {world} ranks')
+        return 2
+    if a.ranks_check:
+        return ranks_check(a, rank, world, local)
 
     import torch
     dist = None
@@ -644,8 +711,10 @@ def main():
     launch_ms = ms / a.steps
     achieved = bytes_launch / (launch_ms / 1e3) / 1e9
     peak, peak_kind = measured_peaks()
+    launch_used = dev.launch()
+    traffic, traffic_src = profile_traffic(a.precision, launch_used, fluid)
     roof = dict(bound='hbm', achieved=achieved, peak=peak, unit='GB/s', frac=achieved / peak,
-                traffic=profile_traffic(a.precision), peak_source=peak_kind,
+                traffic=traffic, traffic_source=traffic_src, peak_source=peak_kind,
                 bytes_per_launch=bytes_launch, launch_ms=launch_ms)
 
     # end to end through the public API with host buffers
@@ -701,10 +770,10 @@ def main():
                dtype=DTYPE[a.precision],
                data=('the reference\'s own Ashburn planes (tests/golden/static10.*)' if wl.get('real') else
                      'synthetic (seeded terrain and buildings; no public dataset involved)'),
-               config=dict(workload=WORKLOADS[a.workload]['desc'], precision=a.precision, arith=a.arith, scheme='pull',
-                           parallelism=f'replicas x{world}', fluid_cells=fluid, l2=f"state {s._dev.info()['state_bytes'] / 1e9:.2f} GB vs 126 MB L2",
-                           launch=dict(block_y=tune[0], zslab=tune[1]) if tune else None,
-                           published=wl.get('published')),
+               config=bench_config(a.workload, a.precision, cells),
+               arith=a.arith, fluid_cells=fluid, replicas=world, state_bytes=s._dev.info()['state_bytes'],
+               launch=dict(block_y=launch_used[0], zslab=launch_used[1], tuned=tune is not None and tune[2] is not None),
+               published=wl.get('published'),
                roofline=roof, cpu_baseline=cpu, e2e=e2e, read_ms=read_ms, gpu_launches=a.steps, clocks=clocks,
                glups_fluid=world * fluid * a.steps / (ms_all / 1e3) / 1e9)
     s.destroy()

@@ -215,14 +215,15 @@ ahx_status ahx_autotune(ahx_handle* h, int steps_per_trial, int* best_block_y, i
 
 /* No counterpart in the reference. The ahx_stats diagnostics (theta, kinetic energy, rho - 1 and fluid-cell sums in
  * FP64, max theta, max |j|/rho, non-finite count) over a state the caller owns, for callers that cannot allocate
- * device memory when they need them: a host recording into a CUDA graph (no cudaMalloc during stream capture), an
- * engine that has given all device memory to its own pool, code that must not block on a driver allocation.
+ * device memory when they need them: an engine that has given all device memory to its own pool, code that must not
+ * block on a driver allocation.
  * f (19N) and g (7N) are f32 device arrays in the reference layout, ktop is the NXY device plane, out is an
  * ahx_stats_out in device memory; the two kernels run on `stream` (a cudaStream_t; NULL = the legacy default stream)
  * and the call returns once they are queued. Nothing is allocated: the per-block partial sums go to one fixed
  * 1 MiB scratch array inside the library (held by every GPU that loads it until the process exits), so grids above
- * 134,217,728 cells are rejected with AHX_EINVAL. The first call on a device resolves that array's address (make it
- * before any stream capture). Calls share the array: two calls that overlap on the GPU race on it. The sums are
+ * 134,217,728 cells are rejected with AHX_EINVAL. The first call on a device (and the first after the device's
+ * context changed, e.g. after cudaDeviceReset) resolves that array's address: make that call before any stream
+ * capture. Calls share the array: two calls that overlap on the GPU race on it. The sums are
  * reduced in a fixed order, so repeated calls on the same state return identical records. */
 ahx_status ahx_stats_noalloc(int nx, int ny, int nz, const float* f, const float* g, const uint32_t* ktop,
                              ahx_stats_out* out, void* stream);

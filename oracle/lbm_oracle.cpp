@@ -30,8 +30,16 @@ namespace {
 
 // Subnormal f32 values are flushed to zero (inputs and results), as the CUDA path does (-ftz=true): the WGSL
 // reference runs with the GPU's f32 denormal mode, where flushing is the norm, and on the CPU subnormal arithmetic
-// would otherwise be orders of magnitude slower. Set in every worker thread before it touches data.
-inline void flush_subnormals() { _mm_setcsr(_mm_getcsr() | 0x8040u); }
+// would otherwise be orders of magnitude slower. Every parallel region holds one of these per thread: it sets
+// flush-to-zero and denormals-are-zero (MXCSR bits 15 and 6) for the region and restores the thread's previous mode
+// when the region ends, so the calling process (numpy, the host metrics) keeps its own floating-point mode.
+struct FlushSubnormals {
+  unsigned saved;
+  FlushSubnormals() : saved(_mm_getcsr()) { _mm_setcsr(saved | 0x8040u); }
+  ~FlushSubnormals() { _mm_setcsr(saved); }
+  FlushSubnormals(const FlushSubnormals&) = delete;
+  FlushSubnormals& operator=(const FlushSubnormals&) = delete;
+};
 
 // lattice tables (kernel.js:19-28); OPP/MIRZ derived as the reference derives them (find the reversed / z-mirrored
 // velocity), weights as the reference's f64 fractions
@@ -455,7 +463,7 @@ void step_all(int nx, int ny, int nz, const void* params, const uint32_t* colv, 
   const Grid<R> G = make_grid<R>(nx, ny, nz, params, colv, ktopc);
 #pragma omp parallel
   {
-    flush_subnormals();
+    const FlushSubnormals ftz;
 #pragma omp for collapse(2) schedule(static)
     for (int k = 0; k < nz; ++k)
       for (int j = 0; j < ny; ++j)
@@ -468,7 +476,10 @@ template <class R>
 void init_all(int nx, int ny, int nz, const void* params, const uint32_t* colv, R* f0, R* f1) {
   const Params P = parse_params(params);
   const long NXY = (long)nx * ny, N = NXY * nz;
-#pragma omp parallel for schedule(static)
+#pragma omp parallel
+  {
+  const FlushSubnormals ftz;
+#pragma omp for schedule(static)
   for (long n = 0; n < N; ++n) {
     const int i = (int)(n % nx), j = (int)((n / nx) % ny), k = (int)(n / NXY);
     const int ktc = (int)colv[4 * ((long)j * nx + i)];
@@ -482,6 +493,7 @@ void init_all(int nx, int ny, int nz, const void* params, const uint32_t* colv, 
       f0[(long)q * N + n] = fq;
       if (f1) f1[(long)q * N + n] = fq;
     });
+  }
   }
 }
 
@@ -530,7 +542,10 @@ void orc_surf_f32(int nx, int ny, int nz, const void* params, const uint32_t* co
                   const float* fA, const float* gA, float conv, float* sout) {
   const Grid<float> G = make_grid<float>(nx, ny, nz, params, colv, ktopc);
   const long NXY = G.NXY;
-#pragma omp parallel for schedule(static)
+#pragma omp parallel
+  {
+  const FlushSubnormals ftz;
+#pragma omp for schedule(static)
   for (long c = 0; c < NXY; ++c) {
     const int i = (int)(c % nx), j = (int)(c / nx);
     const int kg = (int)colv[4 * c + 1];
@@ -554,6 +569,7 @@ void orc_surf_f32(int nx, int ny, int nz, const void* params, const uint32_t* co
     sout[NXY + o] = F.ux * conv;
     sout[2 * NXY + o] = F.uy * conv;
   }
+  }
 }
 
 // genVolWGSL (kernel.js:475-520): theta of the lowest nzv levels, north-up [k][row][col], u8 round(theta*volscale)
@@ -563,7 +579,10 @@ void orc_vol_f32(int nx, int ny, int nz, const void* params, const uint32_t* kto
   const Params P = parse_params(params);
   const long NXY = (long)nx * ny, N = NXY * nz, NVOL = (long)nzv * NXY, NW = (NVOL + 3) / 4;
   float gmax = 0.f;
-#pragma omp parallel for schedule(static) reduction(max : gmax)
+#pragma omp parallel reduction(max : gmax)
+  {
+  const FlushSubnormals ftz;
+#pragma omp for schedule(static)
   for (long t = 0; t < NW; ++t) {
     uint32_t packed = 0;
     float tm = 0.f;
@@ -607,11 +626,13 @@ void orc_vol_f32(int nx, int ny, int nz, const void* params, const uint32_t* kto
     vout[t] = packed;
     gmax = std::max(gmax, std::max(tm, 0.f));
   }
+  }
   *tmax = gmax;
 }
 
 // genReinitWGSL (kernel.js:557-575): cells that turned from solid to fluid get rest equilibrium and theta = 0
 void orc_reinit_f32(int nx, int ny, int nz, const uint32_t* ktopc, const uint32_t* oldk, float* f, float* g) {
+  const FlushSubnormals ftz;
   const long NXY = (long)nx * ny, N = NXY * nz;
   for (long c = 0; c < NXY; ++c) {
     const int k1 = std::min((int)oldk[c], nz);
@@ -630,7 +651,10 @@ void orc_stats_f32(int nx, int ny, int nz, const uint32_t* ktopc, const float* f
   const long NXY = (long)nx * ny, N = NXY * nz;
   double s0 = 0, s1 = 0, s2 = 0, s3 = 0, nonf = 0;
   float tmax = 0.f, umax = 0.f;
-#pragma omp parallel for schedule(static) reduction(+ : s0, s1, s2, s3, nonf) reduction(max : tmax, umax)
+#pragma omp parallel reduction(+ : s0, s1, s2, s3, nonf) reduction(max : tmax, umax)
+  {
+  const FlushSubnormals ftz;
+#pragma omp for schedule(static)
   for (long n = 0; n < N; ++n) {
     const int i = (int)(n % nx), j = (int)((n / nx) % ny), k = (int)(n / NXY);
     if (k < (int)ktopc[(long)j * nx + i]) continue;
@@ -650,6 +674,7 @@ void orc_stats_f32(int nx, int ny, int nz, const uint32_t* ktopc, const float* f
     s3 += 1.0;
     tmax = std::max(tmax, std::max(th, 0.f));
     umax = std::max(umax, std::sqrt(jx * jx + jy * jy + jz * jz) / rho);
+  }
   }
   out[0] = s0;
   out[1] = s1;

@@ -143,11 +143,13 @@ def test_fp64_build_bit_exact_with_fp64_oracle():
     o.destroy()
 
 
-@pytest.mark.parametrize('precision,tol', [('fp16', 2e-3), ('bf16', 2e-2), ('fp16g32', 2e-3), ('bf16g32', 2e-2),
-                                           ('fp16sr', 2e-3)])
+@pytest.mark.parametrize('precision,tol', [('fp16', 1e-3), ('bf16', 2e-2), ('fp16g32', 1e-3), ('bf16g32', 2e-2),
+                                           ('fp16sr', 1e-3)])
 def test_16bit_storage_error_vs_fp64(precision, tol):
     """16-bit population storage (f shifted by w_q and scaled; g likewise, or f32 for the *g32 storages) against
-    the FP64 build after 300 steps with heat on: theta rel-L2 over fluid cells within the stated tolerance."""
+    the FP64 build after 300 steps with heat on: theta rel-L2 over fluid cells within the stated tolerance. The FP16
+    storages are held to the 1e-3 bar of the 16-bit target; BF16 (8 mantissa bits) does not meet that bar and is
+    held to 2e-2 only."""
     met = dict(u10=5.0, dirFrom=250.0, wstar=1.5, blh=700.0)
     h = small_solver(cuda_backend(precision, 'exact'), met=met)
     d = small_solver(cuda_backend('fp64', 'exact'), met=met)
@@ -199,11 +201,12 @@ def test_autotune_keeps_state():
     o.destroy()
 
 
-@pytest.mark.parametrize('shape', [1204, 1304, 1404, 1208, 1308, 504, 404])
-@pytest.mark.parametrize('zslab', [0, 12])
+@pytest.mark.parametrize('shape', [2, 8, 404, 504, 604])
+@pytest.mark.parametrize('zslab', [0, 12, 3])
 def test_launch_shapes_bit_exact(shape, zslab):
-    """Every launch shape of the exact build (TMA-staged kernel: 1000 + 100 x stages + rows; register-budget
-    variants 404 / 504), with whole columns or 12-level z-slabs, stays bit-identical to the oracle."""
+    """The launch shapes the tuner chooses from (2 / 4 / 8 rows per block; register-budget variants 404 / 504 / 604),
+    with whole columns, 12-level or 3-level z-slabs, stay bit-identical to the oracle in the exact build. The
+    TMA-staged kernel is not among them: it is not a tuner candidate."""
     met = dict(u10=5.0, dirFrom=300.0, wstar=1.5, blh=700.0)
     g, o = _pair(met=met)
     g._dev.set_launch(shape, zslab)

@@ -41,3 +41,18 @@ def test_oracle_api30(kat):
     assert r['thetaMax'] == pytest.approx(k['readNoVolNoWind']['thetaMax'], rel=3e-6)
     assert r['simTime'] == pytest.approx(k['readNoVolNoWind']['simTime'], rel=1e-12)
     s.destroy()
+
+
+def test_oracle_restores_the_callers_floating_point_mode():
+    """The oracle flushes f32 subnormals inside its own parallel regions only (as the CUDA build's -ftz=true does);
+    the calling thread keeps gradual underflow afterwards, so host-side metrics computed next to it are unaffected."""
+    from tests.helpers import small_solver
+    tiny = np.array([1e-40], np.float32)
+    assert (tiny * np.float32(1.0))[0] != 0          # subnormals survive before the oracle runs
+    s = small_solver(oracle_backend())
+    s._dbg.stepOut(2).result()
+    s.read(vol=True, wind=True).result()
+    s._dbg.stats()
+    s.destroy()
+    assert (tiny * np.float32(1.0))[0] != 0          # ... and after it
+    assert np.float64(5e-324) * 1.0 != 0

@@ -82,3 +82,33 @@ def test_a_failed_rank_ends_the_other_ranks_collective():
         res = dict(out)
     assert 'injected failure' in res[1]['error']
     assert 'error' in res[0]                                  # rank 0's barrier did not wait for ever
+
+
+def test_bench_gpus_flag_starts_that_many_ranks():
+    """`python bench.py --gpus 2` (the driver's command form, no torchrun around it) starts two ranks itself; the
+    ranks check runs the benchmark's barrier and max-over-ranks reduction (gloo here, no CUDA) and reports both."""
+    import json
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = {k: v for k, v in os.environ.items() if k not in ('RANK', 'WORLD_SIZE', 'LOCAL_RANK', 'MASTER_ADDR',
+                                                            'MASTER_PORT')}
+    r = subprocess.run([sys.executable, os.path.join(root, 'bench.py'), '--gpus', '2', '--ranks-check'],
+                       capture_output=True, text=True, timeout=240, env=env, cwd=root)
+    assert r.returncode == 0, r.stderr[-2000:]
+    line = [x for x in r.stdout.splitlines() if x.startswith('{')]
+    assert len(line) == 1, r.stdout
+    d = json.loads(line[0])
+    assert d['ranks'] == 2 and d['max_rank_seen'] == 1
+
+
+def test_bench_rejects_a_rank_count_other_than_gpus():
+    """Under a launcher whose world size differs from --gpus the benchmark refuses to run instead of reporting a
+    device count it did not use."""
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = dict(os.environ, RANK='0', WORLD_SIZE='1', LOCAL_RANK='0')
+    r = subprocess.run([sys.executable, os.path.join(root, 'bench.py'), '--gpus', '2', '--ranks-check'],
+                       capture_output=True, text=True, timeout=120, env=env, cwd=root)
+    assert r.returncode == 2 and 'ranks' in r.stderr
