@@ -202,8 +202,8 @@ def cpu_baseline(seconds=10.0, max_steps=30, workload='c2'):
 def bench_config(workload, precision, cells):
     """The config dict both arms print for a workload (identical keys and values for the same workload)."""
     return dict(workload=WORKLOADS[workload]['desc'], precision=precision, scheme='pull', parallelism='replicas',
-                l2=f'inputs larger than L2, no flush: state {2 * 26 * cells * CELL_BYTES[precision] / 208 / 1e9:.2f} '
-                   f'GB per replica against a 126 MB L2')
+                l2=f'inputs larger than L2, no flush: state {cells * CELL_BYTES[precision] / 1e9:.2f} GB per replica '
+                   f'(both population buffers) against a 126 MB L2')
 
 
 def run_reference(a, rank):
