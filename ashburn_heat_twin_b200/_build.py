@@ -1,16 +1,17 @@
 """Build libahx.so (the CUDA backend, sm_100a) in-tree with nvcc.
 
 Translation units and their arithmetic flags:
-  step_exact.cu  -fmad=false  fused step, every f32 expression individually rounded (bit-identical to the CPU
-                              restatement of the reference kernels)
-  step_fast.cu   -fmad=true   fused step with multiply-add contraction, approximate division and square root and
-                              the paired collision
+  step_unit.cu      compiled 14 times, once per (arithmetic variant, population storage):
+                    exact  -fmad=false, IEEE division and square root: every f32 expression individually rounded
+                           (bit-identical to the CPU restatement of the reference kernels)
+                    fast   -fmad=true, approximate division and square root, the paired collision
+  step_dispatch.cu  the precision switch of each variant (compiled twice)
   aux.cu         -fmad=false  read-back, init, re-init, stats, layout conversion
   api.cu                      the C ABI (include/ahx.h)
   batch.cu                    batched stepping (ahx_batch_*: tile tables, CUDA graph, stream ordering)
   noalloc.cu                  diagnostics over caller-owned buffers without allocation
-All use -ftz=true (f32 subnormals flushed, as the CPU restatement does); all but step_fast.cu use IEEE division and
-square root.
+All use -ftz=true (f32 subnormals flushed, as the CPU restatement does); all but the fast variant use IEEE division
+and square root.
 """
 from __future__ import annotations
 
@@ -31,14 +32,18 @@ ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
 COMMON = ['-O3', '-std=c++17', '--expt-relaxed-constexpr', '-lineinfo', '-ftz=true', '-Xcompiler', '-fPIC', '-I',
           INCLUDE]
 IEEE = ['-prec-div=true', '-prec-sqrt=true']
-UNITS = {
-    'step_exact.cu': ['-fmad=false'] + IEEE,
-    'step_fast.cu': ['-fmad=true', '-prec-div=false', '-prec-sqrt=false'],
-    'aux.cu': ['-fmad=false'] + IEEE,
-    'api.cu': ['-fmad=false'] + IEEE,
-    'noalloc.cu': ['-fmad=false'] + IEEE,
-    'batch.cu': ['-fmad=false'] + IEEE,
-}
+EXACT = ['-fmad=false'] + IEEE + ['-DAHX_STEP_NS=exact']
+FAST = ['-fmad=true', '-prec-div=false', '-prec-sqrt=false', '-DAHX_STEP_NS=fast', '-DAHX_STEP_FAST=1']
+# (object name, source, flags); the storages are the ahx_precision values 0 .. 6
+UNITS = [(f'step_{v}_p{p}', 'step_unit.cu', flags + [f'-DAHX_STEP_PREC={p}'])
+         for v, flags in (('exact', EXACT), ('fast', FAST)) for p in range(7)] + [
+    ('step_exact_dispatch', 'step_dispatch.cu', EXACT),
+    ('step_fast_dispatch', 'step_dispatch.cu', FAST),
+    ('aux', 'aux.cu', ['-fmad=false'] + IEEE),
+    ('api', 'api.cu', ['-fmad=false'] + IEEE),
+    ('noalloc', 'noalloc.cu', ['-fmad=false'] + IEEE),
+    ('batch', 'batch.cu', ['-fmad=false'] + IEEE),
+]
 
 
 def nvcc():
@@ -61,15 +66,17 @@ def build(force: bool = False, verbose: bool = False, ptxas_v: bool = False) -> 
     cc = nvcc()
 
     def one(unit):
-        obj = os.path.join(OBJDIR, unit.replace('.cu', '.o'))
-        cmd = [cc] + ARCH + COMMON + UNITS[unit] + (['-Xptxas', '-v'] if ptxas_v else []) + \
-            ['-c', os.path.join(CSRC, unit), '-o', obj]
+        name, src, flags = unit
+        obj = os.path.join(OBJDIR, name + '.o')
+        cmd = [cc] + ARCH + COMMON + flags + (['-Xptxas', '-v'] if ptxas_v else []) + \
+            ['-c', os.path.join(CSRC, src), '-o', obj]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
-            raise RuntimeError(f'nvcc failed on {unit}:\n{r.stderr[-6000:]}')
+            raise RuntimeError(f'nvcc failed on {name} ({src}):\n{r.stderr[-6000:]}')
         return obj, r.stderr
 
-    with cf.ThreadPoolExecutor(max_workers=len(UNITS)) as ex:
+    # the longest units (the step instantiations) first
+    with cf.ThreadPoolExecutor(max_workers=max(1, os.cpu_count() or 1)) as ex:
         results = list(ex.map(one, UNITS))
     if verbose or ptxas_v:
         for _, err in results:

@@ -1,6 +1,7 @@
-// Instantiates the fused step kernels for one arithmetic variant. Included once by step_exact.cu and once by
-// step_fast.cu with AHX_STEP_NS set to the variant's namespace; the two translation units are compiled with
-// -fmad=false and -fmad=true respectively.
+// Instantiates the fused step kernels for one arithmetic variant and one population storage. step_unit.cu is compiled
+// once per (variant, storage) with AHX_STEP_NS = exact (-fmad=false) or fast (-fmad=true, AHX_STEP_FAST=1) and
+// AHX_STEP_PREC = the ahx_precision value of the storage, so the 14 instantiation sets compile in parallel; the
+// precision switch of each variant is step_dispatch.cu.
 #pragma once
 
 #include <type_traits>
@@ -119,19 +120,6 @@ static cudaError_t batch_s(const BatchLaunch& B, cudaStream_t s, int* occupancy)
   return batch_m<S, false>(B, s, occupancy);
 }
 
-cudaError_t launch_batch(const BatchLaunch& B, cudaStream_t s, int* occupancy) {
-  switch (B.precision) {
-    case 0: return batch_s<float>(B, s, occupancy);
-    case 1: return batch_s<__half>(B, s, occupancy);
-    case 2: return batch_s<__nv_bfloat16>(B, s, occupancy);
-    case 3: return batch_s<double>(B, s, occupancy);
-    case 4: return batch_s<Mixed<__half, float>>(B, s, occupancy);
-    case 5: return batch_s<Mixed<__nv_bfloat16, float>>(B, s, occupancy);
-    case 6: return batch_s<half_sr>(B, s, occupancy);
-    default: return cudaErrorInvalidValue;
-  }
-}
-
 template <class S, int TY, int DEPTH>
 static cudaError_t launch_tma_t(const DomainView& D, const StepLaunch& L, cudaStream_t s) {
   const int zs = L.zslab > 0 ? L.zslab : D.nz;
@@ -221,18 +209,35 @@ static cudaError_t launch_s(const DomainView& D, const StepLaunch& L, cudaStream
   }
 }
 
-cudaError_t launch_step(const DomainView& D, const StepLaunch& L, cudaStream_t s) {
-  switch (L.precision) {
-    case 0: return launch_s<float>(D, L, s);
-    case 1: return launch_s<__half>(D, L, s);
-    case 2: return launch_s<__nv_bfloat16>(D, L, s);
-    case 3: return launch_s<double>(D, L, s);
-    case 4: return launch_s<Mixed<__half, float>>(D, L, s);
-    case 5: return launch_s<Mixed<__nv_bfloat16, float>>(D, L, s);
-    case 6: return launch_s<half_sr>(D, L, s);
-    default: return cudaErrorInvalidValue;
-  }
+// the storage type of each ahx_precision value
+template <int P>
+struct PrecStorage;
+template <>
+struct PrecStorage<0> { using T = float; };
+template <>
+struct PrecStorage<1> { using T = __half; };
+template <>
+struct PrecStorage<2> { using T = __nv_bfloat16; };
+template <>
+struct PrecStorage<3> { using T = double; };
+template <>
+struct PrecStorage<4> { using T = Mixed<__half, float>; };
+template <>
+struct PrecStorage<5> { using T = Mixed<__nv_bfloat16, float>; };
+template <>
+struct PrecStorage<6> { using T = half_sr; };
+
+#ifdef AHX_STEP_PREC
+#define AHX_PREC_CAT2(a, b) a##b
+#define AHX_PREC_CAT(a, b) AHX_PREC_CAT2(a, b)
+// the entry points of this translation unit's storage, called by the precision switch (step_dispatch.cu)
+cudaError_t AHX_PREC_CAT(launch_step_p, AHX_STEP_PREC)(const DomainView& D, const StepLaunch& L, cudaStream_t s) {
+  return launch_s<typename PrecStorage<AHX_STEP_PREC>::T>(D, L, s);
 }
+cudaError_t AHX_PREC_CAT(launch_batch_p, AHX_STEP_PREC)(const BatchLaunch& B, cudaStream_t s, int* occupancy) {
+  return batch_s<typename PrecStorage<AHX_STEP_PREC>::T>(B, s, occupancy);
+}
+#endif
 
 }  // namespace AHX_STEP_NS
 }  // namespace ahx
