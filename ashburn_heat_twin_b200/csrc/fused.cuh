@@ -469,7 +469,7 @@ __device__ __forceinline__ double sponge_sg_d(const ParamsHead& P, int nz, int k
 // pair, and 1/rho, 1/tau are taken once. Mathematically identical to moments_forces + collide_store; rounding
 // differs (held to the single-step theta rel-L2 <= 1e-5 bar).
 template <class S>
-__device__ __forceinline__ void fast_update(const DomainView& D, const ParamsHead& P,
+__device__ __forceinline__ void fast_update(const DomainView& D, const ParamsHead& P, const RelaxConst& RK,
                                             const Column<RealOf<S>>& C, int k, uint32_t n,
                                             const Cell<RealOf<S>>& X,
                                             Macro<RealOf<S>>& M, uint32_t rs) {
@@ -496,10 +496,10 @@ __device__ __forceinline__ void fast_update(const DomainView& D, const ParamsHea
   const R tb_add = C.spon ? R(C.spg) : R(0);
   Relaxed<R> o;
   lane_relax<R>(
-      P, m, X.g, X.uI, X.vI, X.kb, sg, Fx0, Fy0, Ssrc, tb_add, o,
-      [&](auto Q, R v) {
+      P, RK, m, X.g, X.uI, X.vI, X.kb, sg, Fx0, Fy0, Ssrc, tb_add, o,
+      [&](auto Q, R x) {
         constexpr int q = Q;
-        KF::store(static_cast<StoreF<S>*>(D.dst_f[q]) + n, enc_f_d<KF, q>(v, R(w19(q)), rs));
+        KF::store(static_cast<StoreF<S>*>(D.dst_f[q]) + n, enc_f_x<KF, q>(x, R(w19(q)), rs));
       },
       [&](auto Q, R v) {
         constexpr int q = Q;
@@ -536,18 +536,24 @@ __device__ __forceinline__ float2 pair_load_g(const T* p, uint32_t ps) {
   else
     return make_float2(K::load(p), K::load(p + ps));
 }
+// population P of cells n and n + ps, given as x = f / w (flow) or g (temperature), encoded exactly as the
+// single-cell codec would encode each (enc_f_x / enc_g_d)
 template <int P, class T>
-__device__ __forceinline__ void pair_store_f(T* p, uint32_t ps, float2 v, float w, uint32_t h0, uint32_t h1) {
+__device__ __forceinline__ void pair_store_f(T* p, uint32_t ps, float2 x, float w, uint32_t h0, uint32_t h1) {
   using K = Codec<T>;
-  if constexpr (K::kDither) {
-    const float2 e = vfma(v, vc<float2>(K::kF), vc<float2>(-(double)K::kF * w));
-    K::store(p, K::cvt_sr(e.x, h0 * kDitherMul<P>));
-    K::store(p + ps, K::cvt_sr(e.y, h1 * kDitherMul<P>));
-  } else if constexpr (K::kBytes == 2) {
-    const float2 e = vfma(v, vc<float2>(K::kF), vc<float2>(-(double)K::kF * w));
-    K::store(p, K::cvt(e.x));
-    K::store(p + ps, K::cvt(e.y));
+  if constexpr (K::kBytes == 2) {
+    const float sw = K::kF * w;
+    const float2 e = vfma(x, make_float2(sw, sw), make_float2(-sw, -sw));
+    if constexpr (K::kDither) {
+      const uint32_t d = K::cvt_sr2(e.x, e.y, h0 * kDitherMul<P>, h1 * kDitherMul<P>);
+      K::store_bits(p, d);
+      K::store_bits(p + ps, d >> 16);
+    } else {
+      K::store(p, K::cvt(e.x));
+      K::store(p + ps, K::cvt(e.y));
+    }
   } else {
+    const float2 v = vmul(x, make_float2(w, w));
     K::store(p, v.x);
     K::store(p + ps, v.y);
   }
@@ -557,8 +563,9 @@ __device__ __forceinline__ void pair_store_g(T* p, uint32_t ps, float2 v, uint32
   using K = Codec<T>;
   if constexpr (K::kDither) {
     const float2 e = vmul(v, vc<float2>(K::kG));
-    K::store(p, K::cvt_sr(e.x, h0 * kDitherMul<19 + P>));
-    K::store(p + ps, K::cvt_sr(e.y, h1 * kDitherMul<19 + P>));
+    const uint32_t d = K::cvt_sr2(e.x, e.y, h0 * kDitherMul<19 + P>, h1 * kDitherMul<19 + P>);
+    K::store_bits(p, d);
+    K::store_bits(p + ps, d >> 16);
   } else if constexpr (K::kBytes == 2) {
     const float2 e = vmul(v, vc<float2>(K::kG));
     K::store(p, K::cvt(e.x));
@@ -573,8 +580,9 @@ __device__ __forceinline__ void pair_store_g(T* p, uint32_t ps, float2 v, uint32
 // f32x2 arithmetic. Interior cells are never the first fluid cell (no drag, no source); the result of each lane is
 // bit-identical to stream_interior + fast_update on that cell alone.
 template <class S>
-__device__ __forceinline__ void fast_pair(const DomainView& D, const ParamsHead& P, const float4* prof,
-                                          const Column<float>& C, int k, uint32_t n, uint32_t r0, uint32_t r1) {
+__device__ __forceinline__ void fast_pair(const DomainView& D, const ParamsHead& P, const RelaxConst& RK,
+                                          const float4* prof, const Column<float>& C, int k, uint32_t n, uint32_t r0,
+                                          uint32_t r1) {
   const StoreF<S>* fA = static_cast<const StoreF<S>*>(D.fA);
   const StoreG<S>* gA = static_cast<const StoreG<S>*>(D.gA);
   StoreF<S>* fB = static_cast<StoreF<S>*>(D.fB);
@@ -597,7 +605,7 @@ __device__ __forceinline__ void fast_pair(const DomainView& D, const ParamsHead&
   const float2 tb_add = C.spon ? vc<float2>(C.spg) : zero;
   Relaxed<float2> o;
   lane_relax<float2>(
-      P, m, g, make_float2(p0.x, p1.x), make_float2(p0.y, p1.y), make_float2(p0.z, p1.z),
+      P, RK, m, g, make_float2(p0.x, p1.x), make_float2(p0.y, p1.y), make_float2(p0.z, p1.z),
       make_float2(sponge_sg(P, D.nz, k), sponge_sg(P, D.nz, k + 1)), zero, zero, zero, tb_add, o,
       [&](auto Q, float2 v) {
         constexpr int q = Q;
@@ -671,6 +679,7 @@ __device__ __forceinline__ void step_block(const DomainView& D, int bx, int by, 
   }
   __syncthreads();
   const ParamsHead& P = sP;
+  const RelaxConst RK = relax_const(P);
 
   const int i = bx * kBlockX + threadIdx.x;
   const int j = by * blockDim.y + threadIdx.y;
@@ -725,7 +734,7 @@ __device__ __forceinline__ void step_block(const DomainView& D, int bx, int by, 
         const bool in2 = valid && k >= C.kg && !C.face && k >= C.kint && k + 1 < D.nz - 1;
         const unsigned m2 = __ballot_sync(0xffffffffu, valid && k + 1 >= C.kg);
         if (m2 != 0u && __ballot_sync(0xffffffffu, in2) == m2) {
-          if (in2) fast_pair<S>(D, P, smem_prof, C, k, (uint32_t)k * D.ps + base, seed(k), seed(k + 1));
+          if (in2) fast_pair<S>(D, P, RK, smem_prof, C, k, (uint32_t)k * D.ps + base, seed(k), seed(k + 1));
           ++k;
           continue;
         }
@@ -742,7 +751,7 @@ __device__ __forceinline__ void step_block(const DomainView& D, int bx, int by, 
       else stream_cell<S>(D, P, smem_prof, C, k, n, X);
       Macro<R> M;
       if constexpr (FAST) {
-        fast_update<S>(D, P, C, k, n, X, M, seed(k));
+        fast_update<S>(D, P, RK, C, k, n, X, M, seed(k));
       } else {
         moments_forces<R>(P, C, k, D.nz, X, M);
         collide_store<S>(D, P, C, k, n, X, M, seed(k));

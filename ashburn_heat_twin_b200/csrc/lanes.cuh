@@ -122,15 +122,30 @@ struct Relaxed {
   V Fx, Fy, Fz, ux, uy, uz;
 };
 
+// Parameter-derived constants of the FMA build's relaxation: formed in double precision from the f32 parameters and
+// rounded once to f32, once per block instead of once per cell (the double arithmetic is not free on the GPU).
+struct RelaxConst {
+  float momfac3;   // 3 * momfac
+  float iprt;      // 1 / prt
+};
+__device__ __forceinline__ RelaxConst relax_const(const ParamsHead& P) {
+  return RelaxConst{(float)(3.0 * (double)P.momfac), (float)(1.0 / (double)P.prt)};
+}
+
 // Regularised BGK + Smagorinsky + Guo forcing (secForces / secRelax / secCollision, kernel.js:279-367) and the
 // scalar collision (secScalarCollision, kernel.js:369-386), q paired with its opposite. Fx0, Fy0: drag force (0 away
 // from the ground cell); sg: top-sponge strength (0 below it); Ssrc: heat source (0 off the first fluid cell);
-// tb_add: outflow-sponge addition to the background tau (0 outside it). Each post-collision population is handed to
-// put_f(q, value) / put_g(q, value) as soon as it is formed, so the caller can store it without holding all 26.
+// tb_add: outflow-sponge addition to the background tau (0 outside it). Each post-collision flow population is handed
+// to put_f(q, x) as x = f_q / w_q (the storage codec applies the weight, so a 16-bit codec folds it into its scaled
+// deviation (f - w) s = (x - 1) w s in one multiply-add), each temperature population to put_g(q, g_q), as soon as it
+// is formed, so the caller can store it without holding all 26.
+//
+// With E0 = rho (1 - 1.5 u.u) - 4.5 om trN / 3 - 3 fpre u.F (the rest population's bracket), the bracket of a moving
+// pair (q, opp q) is E0 + cu (4.5 rho cu + 9 fpre cF) + 4.5 om Q:N +- 3 (rho cu + fpre cF).
 template <class V, class PutF, class PutG>
-__device__ __forceinline__ void lane_relax(const ParamsHead& P, const Moments<V>& m, const V (&g)[7], V uI, V vI,
-                                           V kb, V sg, V Fx0, V Fy0, V Ssrc, V tb_add, Relaxed<V>& o, PutF&& put_f,
-                                           PutG&& put_g) {
+__device__ __forceinline__ void lane_relax(const ParamsHead& P, const RelaxConst& K, const Moments<V>& m,
+                                           const V (&g)[7], V uI, V vI, V kb, V sg, V Fx0, V Fy0, V Ssrc, V tb_add,
+                                           Relaxed<V>& o, PutF&& put_f, PutG&& put_g) {
   const V rho = m.rho, irho = m.irho, jx = m.jx, jy = m.jy, jz = m.jz;
   const V rs = vmul(rho, sg);
   const V Fx = vfma(rs, vfma(vneg(jx), irho, uI), Fx0);
@@ -149,11 +164,11 @@ __device__ __forceinline__ void lane_relax(const ParamsHead& P, const Moments<V>
   const V Nyz = vfma(vneg(ruy), uz, m.Pyz);
   const V off2 = vfma(Nyz, Nyz, vfma(Nxz, Nxz, vmul(Nxy, Nxy)));
   const V Pn = vsqrt(vfma(vc<V>(2.0), off2, vfma(Nzz, Nzz, vfma(Nyy, Nyy, vmul(Nxx, Nxx)))));
-  const V tb = vadd(vfma(vc<V>(3.0 * P.momfac), kb, vc<V>(P.tau0)), tb_add);
+  const V tb = vadd(vfma(vc<V>(K.momfac3), kb, vc<V>(P.tau0)), tb_add);
   const V tau = vmul(half, vadd(tb, vsqrt(vfma(tb, tb, vmul(vmul(vc<V>(P.cs2smag), Pn), irho)))));
   const V itau = vrcp(tau);
   const V nusgs = vmul(vsub(tau, tb), vc<V>(1.0 / 3.0));
-  const V kap = vadd(vfma(nusgs, vc<V>(1.0 / P.prt), kb), vc<V>(P.kfloor));
+  const V kap = vadd(vfma(nusgs, vc<V>(K.iprt), kb), vc<V>(P.kfloor));
   const V taug = vfma(vc<V>(4.0), kap, half);
   const V om = vsub(vc<V>(1.0), itau);
   const V fpre = vfma(vc<V>(-0.5), itau, vc<V>(1.0));
@@ -162,16 +177,15 @@ __device__ __forceinline__ void lane_relax(const ParamsHead& P, const Moments<V>
   const V base = vfma(vc<V>(-1.5), usq, vc<V>(1.0));
   const V m3uF = vmul(vc<V>(-3.0), uF);
   const V omtr = vmul(om, trN);
-  {
-    const V w = vc<V>(w19(0));
-    // w rho base - om 4.5 w trN + fpre w (-3 uF)
-    put_f(std::integral_constant<int, 0>{}, vmul(w, vfma(fpre, m3uF, vfma(vc<V>(-4.5), omtr, vmul(rho, base)))));
-  }
+  // rho base - 4.5 om trN - 3 fpre uF: the rest population's bracket and the common part of every other one
+  const V E0 = vfma(fpre, m3uF, vfma(vc<V>(-4.5), omtr, vmul(rho, base)));
+  put_f(std::integral_constant<int, 0>{}, E0);
+  const V r45 = vmul(vc<V>(4.5), rho), f9 = vmul(vc<V>(9.0), fpre), o45 = vmul(vc<V>(4.5), om);
+  const V r3x = vmul(vc<V>(3.0), rho), f3 = vmul(vc<V>(3.0), fpre);
   static_for<9>([&](auto Pi) {
     constexpr int p = Pi;
     constexpr int q = 2 * p + 1;
     constexpr int cx = kC19[q][0], cy = kC19[q][1], cz = kC19[q][2];
-    const V w = vc<V>(w19(q));
     const V cu = vdot<V, cx, cy, cz>(ux, uy, uz);
     const V cF = vdot<V, cx, cy, cz>(Fx, Fy, Fz);
     V qn = vc<V>(0.0);
@@ -186,13 +200,12 @@ __device__ __forceinline__ void lane_relax(const ParamsHead& P, const Moments<V>
     if constexpr (cx != 0 && cy != 0) qn = vfma(vc<V>(2 * cx * cy), Nxy, qn);
     if constexpr (cx != 0 && cz != 0) qn = vfma(vc<V>(2 * cx * cz), Nxz, qn);
     if constexpr (cy != 0 && cz != 0) qn = vfma(vc<V>(2 * cy * cz), Nyz, qn);
-    // even part: w [rho (base + 4.5 cu^2) + 4.5 om (qn - trN) + fpre (9 cu cF - 3 uF)]
-    const V ev = vfma(fpre, vfma(vmul(vc<V>(9.0), cu), cF, m3uF),
-                      vfma(vc<V>(4.5), vfma(om, qn, vneg(omtr)), vmul(rho, vfma(vmul(vc<V>(4.5), cu), cu, base))));
-    // odd part: 3 w (rho cu + fpre cF)
-    const V od = vmul(vc<V>(3.0), vfma(fpre, cF, vmul(rho, cu)));
-    put_f(std::integral_constant<int, q>{}, vmul(w, vadd(ev, od)));
-    put_f(std::integral_constant<int, q + 1>{}, vmul(w, vsub(ev, od)));
+    // even part: E0 + cu (4.5 rho cu + 9 fpre cF) + 4.5 om qn
+    const V ev = vfma(cu, vfma(r45, cu, vmul(f9, cF)), vfma(o45, qn, E0));
+    // odd part: 3 (rho cu + fpre cF)
+    const V od = vfma(r3x, cu, vmul(f3, cF));
+    put_f(std::integral_constant<int, q>{}, vadd(ev, od));
+    put_f(std::integral_constant<int, q + 1>{}, vsub(ev, od));
   });
   const V omg = vrcp(taug);
   const V a = vsub(vc<V>(1.0), omg), one_sg = vsub(vc<V>(1.0), sg);

@@ -142,12 +142,14 @@ struct Codec<__nv_bfloat16> {
 };
 
 // FP16 storage whose step stores round stochastically: the same bits in memory as the __half codec ((f - w) * 16
-// and g * 16), decoded alike, but the fused step encodes each population by adding a pseudo-random 13-bit dither below
-// the 13 mantissa bits an f32 -> f16 conversion drops and truncating, so a value rounds up with probability equal to
-// the dropped fraction (unbiased in the f16 normal range; below 2^-14 the dither covers only part of the dropped bits
-// and rounding leans toward zero). Round-to-nearest keeps a quasi-steady state's rounding error the same step after
-// step, a persistent bias the flow integrates; the dither makes it zero-mean noise. Conversions outside the step (state
-// upload, initialisation) round to nearest like the __half codec.
+// and g * 16), decoded alike, but the fused step encodes each population with Blackwell's stochastic-rounding
+// conversion (cvt.rs.f16x2.f32): a 13-bit dither supplied by the kernel is added below the kept mantissa bits of the
+// magnitude and the result truncated, so a value rounds away from zero with probability equal to the dropped
+// fraction (unbiased, including the f16 subnormal range). The instruction converts two values at once: the low half
+// of its result takes its dither from bits 0-12 of the random operand, the high half from bits 16-28. Round-to-nearest
+// keeps a quasi-steady state's rounding error the same step after step, a persistent bias the flow integrates; the
+// dither makes it zero-mean noise. Conversions outside the step (state upload, initialisation) round to nearest like
+// the __half codec.
 struct half_sr {
   unsigned short x;
 };
@@ -164,10 +166,22 @@ struct Codec<half_sr> {
   }
   __device__ __forceinline__ static float raw(half_sr v) { return __half2float(__ushort_as_half(v.x)); }
   __device__ __forceinline__ static half_sr cvt(float v) { return half_sr{__half_as_ushort(__float2half_rn(v))}; }
-  // r: 32 pseudo-random bits, of which the top 13 are the dither (r >> 19, taken as the high word of r * 2^13 so the
-  // extraction and the add can be one multiply-add)
+  // two values at once: lo with dither bits 16-28 of r_lo, hi with bits 16-28 of r_hi; returns hi << 16 | lo
+  __device__ __forceinline__ static uint32_t cvt_sr2(float lo, float hi, uint32_t r_lo, uint32_t r_hi) {
+    const uint32_t rb = __byte_perm(r_lo, r_hi, 0x7632);   // r_lo[31:16] in the low half, r_hi[31:16] in the high
+    uint32_t d;
+    asm("cvt.rs.f16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(hi), "f"(lo), "r"(rb));
+    return d;
+  }
+  // one value, dither bits 16-28 of r (the same bits cvt_sr2 gives the low half, so a cell converts identically alone
+  // or paired)
   __device__ __forceinline__ static half_sr cvt_sr(float v, uint32_t r) {
-    return half_sr{__half_as_ushort(__float2half_rz(__uint_as_float(__umulhi(r, 0x2000u) + __float_as_uint(v))))};
+    uint32_t d;
+    asm("cvt.rs.f16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(0.0f), "f"(v), "r"(r >> 16));
+    return half_sr{(unsigned short)(d & 0xFFFFu)};
+  }
+  __device__ __forceinline__ static void store_bits(half_sr* p, uint32_t b16) {
+    __stcs(reinterpret_cast<unsigned short*>(p), (unsigned short)b16);
   }
   __device__ __forceinline__ static float dec_f(half_sr v, float w) { return __fmaf_rn(raw(v), 1.0f / kScaleF16, w); }
   __device__ __forceinline__ static float dec_g(half_sr v) { return __fmul_rn(raw(v), 1.0f / kScaleG16); }
@@ -184,8 +198,8 @@ struct Codec<half_sr> {
 
 // Dithers of one cell update: a 32-bit seed from the cell's global index and the step counter through an integer
 // finaliser (the "lowbias32" xorshift-multiply hash published by C. Wellons); population slot p (f: q, g: 19 + q)
-// uses the top 13 bits of seed x M_p, M_p an odd constant per slot (the finaliser of a slot number), so each dither is
-// uniform (x -> x M_p is a bijection) and the 26 products are independent instructions.
+// uses bits 16-28 of seed x M_p, M_p an odd constant per slot (the finaliser of a slot number), so each dither is
+// uniform (x -> x M_p is a bijection of the seed) and the 26 products are independent instructions.
 __host__ __device__ constexpr uint32_t mix32(uint32_t x) {
   x ^= x >> 16;
   x *= 0x7feb352du;
@@ -202,6 +216,20 @@ template <class K, int P, class R>
 __device__ __forceinline__ auto enc_f_d(R v, R w, uint32_t h) {
   if constexpr (K::kDither) return K::enc_f_sr(v, w, h * kDitherMul<P>);
   else return K::enc_f(v, w);
+}
+// encode flow population P given as x = f / w: full-width storages store w x; the 16-bit codecs store
+// (f - w) s = x (s w) - s w, formed by one multiply-add
+template <class K, int P, class R>
+__device__ __forceinline__ auto enc_f_x(R x, R w, uint32_t h) {
+  if constexpr (K::kBytes == 8) {
+    return K::enc_f(__dmul_rn(x, w), w);
+  } else if constexpr (K::kBytes == 4) {
+    return K::enc_f(__fmul_rn(x, w), w);
+  } else {
+    const float e = __fmaf_rn(x, K::kF * w, -(K::kF * w));
+    if constexpr (K::kDither) return K::cvt_sr(e, h * kDitherMul<P>);
+    else return K::cvt(e);
+  }
 }
 template <class K, int P, class R>
 __device__ __forceinline__ auto enc_g_d(R v, uint32_t h) {

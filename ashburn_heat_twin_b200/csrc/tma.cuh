@@ -190,6 +190,7 @@ __device__ __forceinline__ void step_tma_block(const DomainView& D, const TmaMap
   }
   __syncthreads();
   const ParamsHead& P = sP;
+  const RelaxConst RK = relax_const(P);
   const int i = x0 + tx, j = j0 + ty;
   const bool active = i < D.nx && j < D.ny;
   Column<R> C;
@@ -228,7 +229,7 @@ __device__ __forceinline__ void step_tma_block(const DomainView& D, const TmaMap
       }
       Macro<R> Mc;
       if constexpr (FAST) {
-        fast_update<S>(D, P, C, k, n, X, Mc, 0u);
+        fast_update<S>(D, P, RK, C, k, n, X, Mc, 0u);
       } else {
         moments_forces<R>(P, C, k, D.nz, X, Mc);
         collide_store<S>(D, P, C, k, n, X, Mc, 0u);

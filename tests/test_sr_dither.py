@@ -1,8 +1,12 @@
 """The stochastic-rounding dither of AHX_FP16_SR, restated on the CPU (numpy) from its definition: a per-cell seed
 (an xorshift-multiply integer finaliser of the global cell index mixed with the step key), population slot p's
-dither = top 13 bits of seed x M_p (M_p odd), added below the 13 mantissa bits an f32 -> f16 conversion drops, then
-truncation. Checks: each slot's dither is uniform, slots are uncorrelated, and dither + truncation is unbiased in
-the f16 normal range. (The device code itself is checked on the GPU in test_gpu_sr.py.)"""
+dither = bits 16-28 of seed x M_p (M_p odd), which the kernel hands to the stochastic-rounding conversion
+(cvt.rs.f16x2.f32: a two-value instruction that adds its low half's dither from bits 0-12 and its high half's from
+bits 16-28 of the random operand, below the 13 mantissa bits an f32 -> f16 conversion drops, then truncates the
+magnitude). The kernel moves bits 16-31 of each cell's product into the half the conversion reads, so a cell's
+dither is the same whether it is converted alone or paired with the level above. Checks: each slot's dither is
+uniform, slots are uncorrelated, and dither + truncation is unbiased in the f16 normal range. (The device code
+itself is checked on the GPU in test_gpu_sr.py.)"""
 import numpy as np
 
 M32 = 0xFFFFFFFF
@@ -23,7 +27,28 @@ def slot_mul(p):
 
 
 def dithers(seeds, p):
-    return ((seeds * np.uint64(slot_mul(p))) & M32) >> np.uint64(19)
+    return (((seeds * np.uint64(slot_mul(p))) & M32) >> np.uint64(16)) & np.uint64(0x1FFF)
+
+
+def rbits_pair(seed_lo, seed_hi, p):
+    """The random operand of one paired conversion: bits 16-31 of the low cell's product in its low half, of the high
+    cell's in its high half (a byte permutation in the kernel)."""
+    m = np.uint64(slot_mul(p))
+    lo = ((np.asarray(seed_lo, np.uint64) * m) & M32) >> np.uint64(16)
+    hi = ((np.asarray(seed_hi, np.uint64) * m) & M32) >> np.uint64(16)
+    return lo | (hi << np.uint64(16))
+
+
+def test_paired_operand_gives_each_cell_its_own_dither():
+    """The conversion reads bits 0-12 (low value) and 16-28 (high value) of the operand: those are exactly the two
+    cells' single-cell dithers."""
+    rng = np.random.default_rng(5)
+    a = rng.integers(0, 2 ** 32, 1000, dtype=np.uint64)
+    b = rng.integers(0, 2 ** 32, 1000, dtype=np.uint64)
+    for p in (0, 7, 25):
+        r = rbits_pair(a, b, p)
+        assert np.array_equal(r & np.uint64(0x1FFF), dithers(a, p))
+        assert np.array_equal((r >> np.uint64(16)) & np.uint64(0x1FFF), dithers(b, p))
 
 
 def test_slot_multipliers_are_odd_and_distinct():
