@@ -988,7 +988,7 @@ ahx_status ahx_set_launch(ahx_handle* h, int block_y, int zslab) {
     h->prefetch = false;
   } else {
     const int by = block_y % 100, mb = block_y / 100;
-    if (by < 0 || by > 8 || zslab < 0 || (mb != 0 && (mb < 4 || mb > 6)) || (mb && by != 4))
+    if (by < 0 || by > 8 || zslab < 0 || (mb != 0 && (mb < 4 || mb > 6) && mb != 8) || (mb && by != 4))
       return fail(AHX_EINVAL, "live solver: bad launch shape");
     if (block_y || pairs || pf) {
       h->block_y = by ? by : 4;
@@ -1031,9 +1031,12 @@ ahx_status ahx_autotune(ahx_handle* h, int steps_per_trial, int* best_block_y, i
     bool pairs;
   };
   std::vector<Shape> shapes = {{2, 0, 0, 0, false}, {4, 0, 0, 0, false}, {8, 0, 0, 0, false},
-                               {4, 4, 0, 0, false}, {4, 5, 0, 0, false}, {4, 6, 0, 0, false}};
+                               {4, 4, 0, 0, false}, {4, 5, 0, 0, false}, {4, 6, 0, 0, false},
+                               {4, 8, 0, 0, false}};
   if (h->dims.arith == AHX_ARITH_FAST && h->dims.precision != AHX_FP64)
-    for (Shape sh : {Shape{4, 4, 0, 0, true}, Shape{4, 5, 0, 0, true}, Shape{4, 6, 0, 0, true}}) shapes.push_back(sh);
+    for (Shape sh : {Shape{4, 4, 0, 0, true}, Shape{4, 5, 0, 0, true}, Shape{4, 6, 0, 0, true},
+                     Shape{4, 8, 0, 0, true}})
+      shapes.push_back(sh);
   // The TMA-staged kernel is not a candidate: it never won a trial (16-20 against 26.6 GLUPS on 600x600x64) and an
   // early build of it once stopped with a misaligned-address error whose cause was not found. It stays reachable only
   // through an explicit ahx_set_launch value.

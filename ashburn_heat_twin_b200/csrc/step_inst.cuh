@@ -17,8 +17,8 @@ namespace AHX_STEP_NS {
 #define AHX_STEP_FAST 0
 #endif
 
-// MINB = 0: up to 256 threads per block, registers as the compiler likes; MINB = 4 / 5 / 6: 128-thread blocks with
-// 4 / 5 / 6 resident per SM (a 128 / 96 / 80 register budget), chosen by the launch-shape tuner
+// MINB = 0: up to 256 threads per block, registers as the compiler likes; MINB = 4 / 5 / 6 / 8: 128-thread blocks
+// with that many resident per SM (a 128 / 96 / 80 / 64 register budget), chosen by the launch-shape tuner
 // Stochastic-rounding storages: a block (tile) of a step reports done; the last of the step's `blocks` to do so
 // advances the step counter the next step's dithers are keyed on (every block read it before reporting).
 __device__ __forceinline__ void tick_done(const DomainView& D, uint32_t blocks) {
@@ -171,6 +171,7 @@ static cudaError_t launch_t(const DomainView& D, const StepLaunch& L, cudaStream
         case 4: step_kernel<S, 0, false, 4, true><<<grid, block, smem, s>>>(D, zs); return cudaGetLastError();
         case 5: step_kernel<S, 0, false, 5, true><<<grid, block, smem, s>>>(D, zs); return cudaGetLastError();
         case 6: step_kernel<S, 0, false, 6, true><<<grid, block, smem, s>>>(D, zs); return cudaGetLastError();
+        case 8: step_kernel<S, 0, false, 8, true><<<grid, block, smem, s>>>(D, zs); return cudaGetLastError();
         default: step_kernel<S, 0, false, 0, true><<<grid, block, smem, s>>>(D, zs); return cudaGetLastError();
       }
     }
@@ -186,6 +187,10 @@ static cudaError_t launch_t(const DomainView& D, const StepLaunch& L, cudaStream
     }
     if (minb == 6) {
       step_kernel<S, MODE, BUDGET, 6><<<grid, block, smem, s>>>(D, zs);
+      return cudaGetLastError();
+    }
+    if (minb == 8) {
+      step_kernel<S, MODE, BUDGET, 8><<<grid, block, smem, s>>>(D, zs);
       return cudaGetLastError();
     }
   }

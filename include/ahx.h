@@ -201,7 +201,7 @@ ahx_status ahx_accum_read(ahx_handle* h, double* surf3, double* faces, int64_t* 
 /* --- tuning ----------------------------------------------------------------------------------------------------- */
 
 /* launch shape of the fused step: block_y = threads per block in y (x is one warp) plus 100 x the register-budget
- * variant (0: compiler's choice; 4, 5 or 6: 128-thread blocks, that many resident per SM, only with block_y 4), plus
+ * variant (0: compiler's choice; 4, 5, 6 or 8: 128-thread blocks, that many resident per SM, only with block_y 4), plus
  * 2000 for paired levels (two interior levels per thread on packed f32x2 arithmetic; FMA build, f32 arithmetic; the
  * results are bit-identical to unpaired), plus 10000 for an L2 prefetch of the next level's source rows (FMA build;
  * a hint that changes no result); or, for the TMA-staged kernel, 1000 + 100 x stages + rows (rows 4 with 2-4 stages,
