@@ -10,6 +10,7 @@ Translation units and their arithmetic flags:
   api.cu                      the C ABI (include/ahx.h)
   batch.cu                    batched stepping (ahx_batch_*: tile tables, CUDA graph, stream ordering)
   noalloc.cu                  diagnostics over caller-owned buffers without allocation
+  server.cu                   the serving scheduler thread (ahx_server_*: admission, batched chunks, read-back)
 All use -ftz=true (f32 subnormals flushed, as the CPU restatement does); all but the fast variant use IEEE division
 and square root.
 """
@@ -43,6 +44,7 @@ UNITS = [(f'step_{v}_p{p}', 'step_unit.cu', flags + [f'-DAHX_STEP_PREC={p}'])
     ('api', 'api.cu', ['-fmad=false'] + IEEE),
     ('noalloc', 'noalloc.cu', ['-fmad=false'] + IEEE),
     ('batch', 'batch.cu', ['-fmad=false'] + IEEE),
+    ('server', 'server.cu', ['-fmad=false'] + IEEE),
 ]
 
 

@@ -27,7 +27,8 @@ SYMBOLS = ('ahx_create', 'ahx_destroy', 'ahx_last_error', 'ahx_get_info', 'ahx_s
            'ahx_budget_enable', 'ahx_budget_read', 'ahx_set_launch', 'ahx_autotune', 'ahx_time_steps', 'ahx_stats_noalloc',
            'ahx_batch_create', 'ahx_batch_step', 'ahx_batch_time_steps', 'ahx_batch_sync', 'ahx_batch_set_launch',
            'ahx_batch_get_info', 'ahx_batch_destroy', 'ahx_batch_set_members', 'ahx_accum_enable', 'ahx_accum_read',
-           'ahx_set_slab', 'ahx_row_bytes', 'ahx_row_pack', 'ahx_row_unpack')
+           'ahx_set_slab', 'ahx_row_bytes', 'ahx_row_pack', 'ahx_row_unpack', 'ahx_server_create',
+           'ahx_server_submit', 'ahx_server_poll', 'ahx_server_stats', 'ahx_server_destroy')
 
 
 class AhxError(RuntimeError):
@@ -52,6 +53,36 @@ class StatsOut(ctypes.Structure):
     _fields_ = [('sum_theta', ctypes.c_double), ('sum_ke', ctypes.c_double), ('sum_rho_dev', ctypes.c_double),
                 ('count', ctypes.c_double), ('theta_max', ctypes.c_float), ('umax', ctypes.c_float),
                 ('non_finite', ctypes.c_uint32), ('pad', ctypes.c_uint32)]
+
+
+class ServerConfig(ctypes.Structure):
+    _fields_ = [('device_ordinal', ctypes.c_int32), ('precision', ctypes.c_int32), ('arith', ctypes.c_int32),
+                ('chunk', ctypes.c_int32), ('max_cells', ctypes.c_int64), ('hbm_budget_bytes', ctypes.c_uint64),
+                ('batch_mode', ctypes.c_int32), ('tune', ctypes.c_int32), ('depth', ctypes.c_int32),
+                ('pad', ctypes.c_int32)]
+
+
+class RequestIn(ctypes.Structure):
+    _fields_ = [('nx', ctypes.c_int32), ('ny', ctypes.c_int32), ('nz', ctypes.c_int32), ('steps', ctypes.c_int32),
+                ('params', ctypes.c_void_p), ('params_bytes', ctypes.c_size_t), ('colv', ctypes.c_void_p),
+                ('ktop', ctypes.c_void_p), ('conv', ctypes.c_float), ('volscale', ctypes.c_float),
+                ('nzv', ctypes.c_int32), ('want_vol', ctypes.c_int32), ('want_wind', ctypes.c_int32),
+                ('pad', ctypes.c_int32), ('user_tag', ctypes.c_uint64)]
+
+
+class ServerResult(ctypes.Structure):
+    _fields_ = [('ticket', ctypes.c_uint64), ('user_tag', ctypes.c_uint64), ('nx', ctypes.c_int32),
+                ('ny', ctypes.c_int32), ('nz', ctypes.c_int32), ('nzv', ctypes.c_int32), ('steps', ctypes.c_int32),
+                ('status', ctypes.c_int32), ('submitted_s', ctypes.c_double), ('admitted_s', ctypes.c_double),
+                ('done_s', ctypes.c_double), ('theta_max', ctypes.c_float), ('want_vol', ctypes.c_int32),
+                ('want_wind', ctypes.c_int32), ('pad', ctypes.c_int32)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_int64) for k in ('submitted', 'admitted', 'completed', 'queued', 'active',
+                                               'cell_updates', 'chunks', 'batch_steps', 'slots', 'idle_slots',
+                                               'evictions', 'resident_cells')] + \
+        [('slot_bytes', ctypes.c_uint64), ('hbm_budget_bytes', ctypes.c_uint64), ('elapsed_s', ctypes.c_double)]
 
 
 class BudgetOut(ctypes.Structure):
@@ -123,6 +154,11 @@ def load_library(path: str = LIB_PATH):
         'ahx_accum_read': [H, vp, vp, ctypes.POINTER(ctypes.c_int64), i],
         'ahx_batch_get_info': [H, ctypes.POINTER(BatchInfoOut)],
         'ahx_batch_destroy': [H],
+        'ahx_server_create': [ctypes.POINTER(ServerConfig), ctypes.POINTER(H)],
+        'ahx_server_submit': [H, ctypes.POINTER(RequestIn), u64p],
+        'ahx_server_poll': [H, ctypes.c_uint64, i, ctypes.POINTER(ServerResult), vp, vp, vp, vp],
+        'ahx_server_stats': [H, ctypes.POINTER(ServerStats)],
+        'ahx_server_destroy': [H],
     }
     for name, args in sig.items():
         fn = getattr(L, name)
@@ -453,3 +489,68 @@ class Batch:
         if self.b is not None:
             self._call('ahx_batch_destroy', self.b)
             self.b = None
+
+
+class Server:
+    """Owner of one ahx_server (include/ahx.h): the continuous-batching scheduler thread inside libahx.so. submit()
+    copies a request's byte images in and returns its ticket; poll() returns (result info, surf, u, v, vol) once the
+    request is answered, or None while it is not (timeout)."""
+
+    MODES = {'branches': 0, 'persistent': 1}
+
+    def __init__(self, device=None, precision='fp32', arith='fast', chunk=256, max_cells=24_000_000,
+                 hbm_budget_bytes=0, batch_mode='branches', tune=True, depth=2):
+        self.L = load_library()
+        cfg = ServerConfig(device_ordinal=-1 if device is None else int(device), precision=PRECISIONS[precision],
+                           arith=ARITH[arith], chunk=int(chunk), max_cells=int(max_cells),
+                           hbm_budget_bytes=int(hbm_budget_bytes or 0), batch_mode=self.MODES[batch_mode],
+                           tune=int(bool(tune)), depth=int(depth), pad=0)
+        h = ctypes.c_void_p()
+        self._call('ahx_server_create', ctypes.byref(cfg), ctypes.byref(h))
+        self.h = h
+        self.cfg = cfg
+
+    def _call(self, name, *args):
+        st = getattr(self.L, name)(*args)
+        if st != 0:
+            raise AhxError(st, self.L.ahx_last_error().decode(errors='replace'))
+
+    def submit(self, nx, ny, nz, steps, params, colv, ktop, conv, volscale, nzv, want_vol=True, want_wind=True,
+               tag=0):
+        pa = np.frombuffer(bytes(params), np.uint8)
+        cv = np.ascontiguousarray(colv, np.uint32).ravel()
+        kt = np.ascontiguousarray(ktop, np.uint32).ravel()
+        if cv.size != 4 * nx * ny or kt.size != nx * ny:
+            raise ValueError('column records or ktop plane of the wrong size')
+        q = RequestIn(nx=int(nx), ny=int(ny), nz=int(nz), steps=int(steps), params=pa.ctypes.data,
+                      params_bytes=pa.size, colv=cv.ctypes.data, ktop=kt.ctypes.data, conv=float(conv),
+                      volscale=float(volscale), nzv=int(nzv), want_vol=int(bool(want_vol)),
+                      want_wind=int(bool(want_wind)), pad=0, user_tag=int(tag))
+        t = ctypes.c_uint64()
+        self._call('ahx_server_submit', self.h, ctypes.byref(q), ctypes.byref(t))
+        return t.value
+
+    def poll(self, ticket, timeout_ms=0, nx=None, ny=None, nzv=None, want_vol=True, want_wind=True):
+        NXY = int(nx) * int(ny)
+        surf = np.empty(NXY, np.float32)
+        u = np.empty(NXY, np.float32) if want_wind else None
+        v = np.empty(NXY, np.float32) if want_wind else None
+        vol = np.empty(int(nzv) * NXY, np.uint8) if want_vol else None
+        info = ServerResult()
+        st = self.L.ahx_server_poll(self.h, ctypes.c_uint64(ticket), int(timeout_ms), ctypes.byref(info), _ptr(surf),
+                                    _ptr(u), _ptr(v), _ptr(vol))
+        if st == 5:
+            return None
+        if st != 0:
+            raise AhxError(st, self.L.ahx_last_error().decode(errors='replace'))
+        return info, surf, u, v, vol
+
+    def stats(self):
+        o = ServerStats()
+        self._call('ahx_server_stats', self.h, ctypes.byref(o))
+        return {k: getattr(o, k) for k, _ in ServerStats._fields_}
+
+    def destroy(self):
+        if self.h is not None:
+            self._call('ahx_server_destroy', self.h)
+            self.h = None

@@ -1,21 +1,27 @@
 """Serving loop with continuous batching over the live solver.
 
 A request is one scenario of the live page (js/live.js drives one at a time: setMet, setExistingFlux,
-setNewCampuses, then step until a simulated time, then read()). The server runs many at once on one device:
+setNewCampuses, then step until a simulated time, then read()). The server runs many at once on one device.
 
+NativeServer (the default, `Server`): the scheduler is the C ABI server inside libahx.so (ahx_server_*). The host side
+here builds each request's byte images exactly as a fresh solver would upload them (a LiveSolver over a recording
+device replays setMet / setExistingFlux / setNewCampuses / resetFlow) and submits them when the request arrives; the
+library admits requests under a resident-cell budget and the device-memory budget, steps the active ones together in
+batched chunks (continuous batching: the member list changes between chunks) and answers each with its read-back.
+
+HostServer: the same policy as a Python loop over LiveBatch (or any batch object with the LiveBatch protocol), for
+backends without the C ABI server (the CPU oracle in host-logic tests):
 - admission: an arrived request takes a solver slot of its grid class (a recycled one, or a new one while the
   device-memory budget allows) as long as the resident cells stay under `max_cells`; otherwise it queues (FIFO);
 - a slot is configured exactly like a fresh page would be: setMet, setExistingFlux, setNewCampuses, resetFlow;
-- the active slots are stepped together by one LiveBatch in chunks of at most `chunk` steps, never past any
-  member's remaining steps: by default each slot's own tuned step kernel on parallel branches of one CUDA graph per
-  two steps (the device runs the branches concurrently), or one persistent launch per step over all slots' tiles;
-  the member list follows the active slots at chunk boundaries (continuous batching);
+- the active slots are stepped together by one batch in chunks of at most `chunk` steps, never past any member's
+  remaining steps; the member list follows the active slots at chunk boundaries;
 - chunks are queued ahead (up to `depth` in flight) so admission, set-up uploads and read-back overlap the device;
 - a finished request is answered with read() (surface theta, u, v and the u8 volume) and its slot returns to the
   pool of its class once that read has arrived.
 
 Each request's answer is bit-identical to running its scenario alone on a fresh solver (the batched step is).
-The reference has no server; this is the host-side scheduler over the batched C ABI (ahx_batch_*).
+The reference has no server.
 """
 from __future__ import annotations
 
@@ -68,8 +74,8 @@ def _state_bytes(solver):
 DEFAULT_BATCH_LAUNCH = dict(use_graph='branches')
 
 
-class Server:
-    """Continuous-batching server on one device. `backend` builds a solver's device (CudaDevice by default);
+class HostServer:
+    """Continuous-batching server on one device, scheduled by this Python loop. `backend` builds a solver's device (CudaDevice by default);
     `batch_factory(solvers)` returns an object with step(n) -> Pending, set_members(solvers) and destroy()
     (LiveBatch by default); `batch_launch` holds its set_launch keywords (DEFAULT_BATCH_LAUNCH with LiveBatch, none
     with another factory unless given). `tune_slots` runs the launch-shape tuner on the first slot of each grid class
@@ -359,3 +365,174 @@ class SequentialBatch:
 
     def destroy(self):
         self.solvers = []
+
+
+class ImageRecorder:
+    """A device for LiveSolver that keeps the byte images the solver uploads (parameter block, column records, ktop
+    plane) instead of running anything: the host half of a request whose device half is the C ABI server."""
+
+    adapter = 'image recorder (no device)'
+
+    def __init__(self, nx, ny, nz):
+        self.nx, self.ny, self.nz = nx, ny, nz
+        self.params = None
+        self.colv = None
+        self.ktop = None
+
+    def set_params(self, b):
+        self.params = bytes(b)
+
+    def set_columns(self, colv):
+        self.colv = np.array(colv, np.uint32, copy=True)
+
+    def set_ktop(self, ktop, old=None):
+        self.ktop = np.array(ktop, np.uint32, copy=True)
+
+    def init_flow(self):
+        pass
+
+    def clear_heat(self):
+        pass
+
+    def set_parity(self, p):
+        pass
+
+    def sync(self):
+        pass
+
+    def lost(self):
+        return None
+
+    def fence(self):
+        return S.Pending(value=None)
+
+    def step(self, n, mode):
+        raise S.LiveSolverError('live solver: an image recorder does not step')
+
+    def destroy(self):
+        pass
+
+
+class NativeServer:
+    """Continuous batching by the C ABI server (ahx_server_*). `run(requests)` replays a trace in real time: each
+    request's images are built and submitted at its arrival time, answers are collected as the server finishes them.
+    The request objects get `admitted` / `done` (seconds after the run started), `steps`, `cells` and `result` (the
+    read() dict a solver would return: simTime, surf, u, v, vol, volMax, nzv, thetaMax, heatMW, steps)."""
+
+    def __init__(self, static, precision='fp32', arith='fast', device=None, max_cells=24_000_000, chunk=256,
+                 hbm_budget_bytes=None, batch_mode='branches', tune=True, depth=2, u10Max=8.0, volMax=3.0,
+                 clock=time.perf_counter, sleep=time.sleep):
+        from .cuda_device import Server as CServer
+        self.static = static
+        self.u10Max = u10Max
+        self.volMax = float(volMax)
+        self.clock, self.sleep = clock, sleep
+        self.srv = CServer(device=device, precision=precision, arith=arith, chunk=chunk, max_cells=max_cells,
+                           hbm_budget_bytes=hbm_budget_bytes or 0, batch_mode=batch_mode, tune=tune, depth=depth)
+        self.templates: dict = {}      # grid class -> LiveSolver over an ImageRecorder
+        self.batch_launch = dict(mode=batch_mode, tune=bool(tune))
+        self.max_cells, self.chunk = int(max_cells), int(chunk)
+        self.hbm_budget = self.srv.stats()['hbm_budget_bytes']
+        self.host_s = 0.0              # host time spent building images
+
+    def images(self, r: Request):
+        """The byte images and read-back settings a fresh solver configured for r would use."""
+        key = (r.dx, r.heightM)
+        s = self.templates.get(key)
+        if s is None:
+            s = S.create_live_solver(backend=ImageRecorder, static=self.static, dx=r.dx, allowAnyDx=True,
+                                     heightM=r.heightM, u10Max=self.u10Max, met=r.met, existingFlux=r.flux)
+            self.templates[key] = s
+        s.setMet(r.met)
+        s.setExistingFlux(r.flux)
+        s.setNewCampuses([r.campus])
+        s.resetFlow()
+        rec = s._dev
+        dt = s.info['dt']
+        return dict(nx=s.info['nx'], ny=s.info['ny'], nz=s.info['nz'], params=rec.params, colv=rec.colv,
+                    ktop=rec.ktop, conv=np.float32(s._conv), volscale=np.float32(255 / self.volMax), nzv=s.nzv, dt=dt,
+                    heatMW=s._heatMW, steps=int(math.ceil(r.sim_s / dt - 1e-9)))
+
+    def submit(self, r: Request):
+        t = self.clock()
+        im = self.images(r)
+        self.host_s += self.clock() - t
+        r.steps = im['steps']
+        r.cells = im['nx'] * im['ny'] * im['nz']
+        ticket = self.srv.submit(im['nx'], im['ny'], im['nz'], r.steps, im['params'], im['colv'], im['ktop'],
+                                 im['conv'], im['volscale'], im['nzv'], True, True, tag=r.id)
+        return ticket, im
+
+    def _collect(self, ticket, im, r, t0, offset, timeout_ms=0):
+        got = self.srv.poll(ticket, timeout_ms, im['nx'], im['ny'], im['nzv'], True, True)
+        if got is None:
+            return False
+        info, surf, u, v, vol = got
+        r.done = self.clock() - t0
+        r.admitted = info.admitted_s - offset
+        r.result = dict(simTime=r.steps * im['dt'], surf=surf, u=u, v=v, vol=vol, volMax=self.volMax, nzv=im['nzv'],
+                        thetaMax=float(info.theta_max), heatMW=im['heatMW'], steps=r.steps)
+        return True
+
+    def run(self, requests, timeout_s=None):
+        """Serve `requests` in real time (arrival times relative to the call); returns the statistics dict. Raises
+        TimeoutError if the trace is not finished within timeout_s seconds (None: no bound)."""
+        reqs = sorted(requests, key=lambda r: r.arrival)
+        st0 = self.srv.stats()
+        t0 = self.clock()
+        offset = st0['elapsed_s'] + (self.clock() - t0)   # server clock at the run's start (to within a poll)
+        nxt = 0
+        open_: list = []
+        done = 0
+        while done < len(reqs):
+            now = self.clock() - t0
+            if timeout_s is not None and now > timeout_s:
+                raise TimeoutError(f'serving: {done} of {len(reqs)} requests answered after {now:.1f} s')
+            while nxt < len(reqs) and reqs[nxt].arrival <= now:
+                r = reqs[nxt]
+                ticket, im = self.submit(r)
+                open_.append((ticket, im, r))
+                nxt += 1
+            keep = []
+            for item in open_:
+                if self._collect(item[0], item[1], item[2], t0, offset):
+                    done += 1
+                else:
+                    keep.append(item)
+            open_ = keep
+            if done < len(reqs):
+                wait = reqs[nxt].arrival - (self.clock() - t0) if nxt < len(reqs) else 0.002
+                if open_ and not (nxt < len(reqs) and wait <= 0):
+                    # block on the oldest open request until the next arrival (bounded)
+                    ms = int(max(0.0, min(wait, 0.002)) * 1000)
+                    ticket, im, r = open_[0]
+                    if self._collect(ticket, im, r, t0, offset, timeout_ms=ms):
+                        done += 1
+                        open_.pop(0)
+                elif not open_ and wait > 0:
+                    self.sleep(min(wait, 0.01))
+        makespan = self.clock() - t0
+        st1 = self.srv.stats()
+        lat = np.array([r.done - r.arrival for r in reqs])
+        qd = np.array([r.admitted - r.arrival for r in reqs])
+        upd = st1['cell_updates'] - st0['cell_updates']
+        return dict(requests=len(reqs), makespan_s=makespan, cell_updates=int(upd),
+                    glups=upd / makespan / 1e9 if makespan > 0 else 0.0,
+                    latency_p50_s=float(np.percentile(lat, 50)), latency_p99_s=float(np.percentile(lat, 99)),
+                    latency_mean_s=float(lat.mean()), queue_p50_s=float(np.percentile(qd, 50)),
+                    queue_p99_s=float(np.percentile(qd, 99)), chunks=st1['chunks'] - st0['chunks'],
+                    batch_steps=st1['batch_steps'] - st0['batch_steps'], slots=st1['slots'],
+                    slot_bytes=st1['slot_bytes'], evictions=st1['evictions'] - st0['evictions'],
+                    host_image_s=self.host_s)
+
+    def stats(self):
+        return self.srv.stats()
+
+    def close(self):
+        for s in self.templates.values():
+            s.destroy()
+        self.templates = {}
+        self.srv.destroy()
+
+
+Server = NativeServer

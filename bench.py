@@ -352,12 +352,49 @@ def main_batch(a, rank, world, local, dist, torch):
     return 0
 
 
+def serve_serial(st, reqs, backend, tuned, clock=time.perf_counter):
+    """The serial arm of the serving comparison, run for real: the same requests in arrival order, each solved alone
+    end to end through the public API of one solver per grid class (setMet, setExistingFlux, setNewCampuses,
+    resetFlow, step(n), read()), a request starting when it has arrived and the previous one has been answered.
+    Returns (latencies, makespan, cell updates)."""
+    from ashburn_heat_twin_b200 import solver as S
+    solvers = {}
+    for r in reqs:
+        key = (r.dx, r.heightM)
+        if key not in solvers:
+            s = S.create_live_solver(backend=backend, static=st, dx=r.dx, allowAnyDx=True, heightM=r.heightM,
+                                     u10Max=8, met=r.met, existingFlux=r.flux)
+            if key in tuned:
+                s._dev.set_launch(*tuned[key])
+            solvers[key] = s
+    lat, upd = [], 0
+    t0 = clock()
+    for r in sorted(reqs, key=lambda r: r.arrival):
+        wait = r.arrival - (clock() - t0)
+        if wait > 0:
+            time.sleep(wait)
+        s = solvers[(r.dx, r.heightM)]
+        s.setMet(r.met)
+        s.setExistingFlux(r.flux)
+        s.setNewCampuses([r.campus])
+        s.resetFlow()
+        n = int(math.ceil(r.sim_s / s.info['dt'] - 1e-9))
+        s.step(n)
+        s.read(vol=True, wind=True).result()
+        lat.append(clock() - t0 - r.arrival)
+        upd += n * s.info['nCells']
+    makespan = clock() - t0
+    for s in solvers.values():
+        s.destroy()
+    return lat, makespan, upd
+
+
 def main_serve(a, rank, world, local, dist, torch):
-    """The serving workload: a seeded Poisson trace of requests served with continuous batching (the admitted
-    requests' own tuned step kernels on parallel branches of one graph per two steps, or with --batch-mode persistent
-    one persistent launch per step over all of them; chunks of --chunk steps, admission under a cell budget). Reports the
-    aggregate served rate, latency percentiles and queueing delay, and the same trace solved back to back (FIFO, each
-    request alone at its class's measured solo rate)."""
+    """The serving workload: a seeded Poisson trace of requests served by the C ABI server (ahx_server_*: continuous
+    batching, admission by resident cells and free HBM, chunks of --chunk steps; each request's own tuned step kernel
+    on parallel graph branches, or --batch-mode persistent). The served rate is end to end (host image building,
+    uploads, batched steps and read-back inside the wall clock). The serial arm runs the same trace for real: every
+    request alone through the public solver API, back to back in arrival order, set-up and read-back included."""
     import numpy as np
 
     from ashburn_heat_twin_b200 import scenarios as SC
@@ -369,86 +406,76 @@ def main_serve(a, rank, world, local, dist, torch):
     def backend(nx, ny, nz):
         return CudaDevice(nx, ny, nz, device=local, precision=a.precision, arith=a.arith)
 
-    # warm pool: idle slots of every class in the mix's proportions up to the cell budget, then a short trace
-    # through the same server (kernels, graph capture, read-back staging)
-    # admission by free device memory (80 % of what is free now) as well as by the resident-cell budget
     free_b, _ = torch.cuda.mem_get_info(local)
-    if a.batch_minb or a.batch_zslab or a.batch_mode == 'persistent':
-        blaunch = dict(minb=a.batch_minb or 5, zslab=a.batch_zslab or 8)
-    else:
-        blaunch = dict(use_graph='branches')
-    srv = SV.Server(st, backend=backend, max_cells=a.max_cells, chunk=a.chunk, hbm_budget_bytes=int(0.8 * free_b),
-                    batch_launch=blaunch)
-    per_req = sum(sh * (6000 // dx) ** 2 * round(hm / dx) for sh, dx, hm in SC.SERVE_MIX)
-    for sh, dx, hm in SC.SERVE_MIX:
-        tmpl = SV.Request(id=-1, arrival=0.0, dx=dx, heightM=hm, met=dict(synth.C1_MET), flux=400.0,
-                          campus=dict(id='W', mw=0.0, halls=[]))
-        srv.prewarm(tmpl, int(math.ceil(sh * a.max_cells / per_req)) + 1)
-    warm = SV.requests_from_trace(SC.serve_trace(st, 6, 1000.0, seed=a.seed + 100), sim_s=5.0)
-    srv.run(warm, timeout_s=300)
-    srv.cell_updates = srv.launch_chunks = srv.rebuilds = srv.evictions = srv.batch_steps = 0
+    srv = SV.NativeServer(st, precision=a.precision, arith=a.arith, device=local, max_cells=a.max_cells,
+                          chunk=a.chunk, hbm_budget_bytes=int(0.8 * free_b), batch_mode=a.batch_mode, tune=True)
+    # warm-up through the same server: slots of every class, launch tuning, graph capture, read-back staging
+    warm = SV.requests_from_trace(SC.serve_trace(st, 12, 1000.0, seed=a.seed + 100), sim_s=5.0)
+    srv.run(warm, timeout_s=600)
     # each rank serves its own trace (replicas: seed + rank); the job's rate is all ranks' cell updates over the
     # longest makespan
-    reqs = SV.requests_from_trace(SC.serve_trace(st, a.requests, a.rate, seed=a.seed + rank), sim_s=SC.SERVE_SIM_S)
+    trace = SC.serve_trace(st, a.requests, a.rate, seed=a.seed + rank)
+    reqs = SV.requests_from_trace(trace, sim_s=SC.SERVE_SIM_S)
     if dist is not None:
         dist.barrier()
-    srv.chunk_log = []
     with Clocks(local) as clk:
-        stats = srv.run(reqs, timeout_s=900)
+        stats = srv.run(reqs, timeout_s=3600)
     clocks = clk.summary()
     makespan_all = RP.max_over_ranks(stats['makespan_s'], dist, f'cuda:{local}')
     job_glups = RP.aggregate_rate(stats['cell_updates'], world, makespan_all) / 1e9
-    # device-busy estimate from the chunk completions the host observed (queue depth keeps the device fed)
-    busy, last = 0.0, 0.0
-    for issued, k, cells_, members, fin in srv.chunk_log:
-        if fin == fin:
-            busy += max(0.0, fin - max(last, issued))
-            last = fin
-    log(f'[rank {rank}] serving: {len(srv.chunk_log)} chunks, observed busy {busy:.2f} s of '
-        f'{stats["makespan_s"]:.2f} s; first chunks: ' +
-        '; '.join(f'{c[1]} steps x {c[2] / 1e6:.1f} M cells ({c[3]} req) {c[0]:.2f}->{c[4]:.2f}s'
-                  for c in srv.chunk_log[:6]) + ' ... last: ' +
-        '; '.join(f'{c[1]} steps x {c[2] / 1e6:.1f} M cells ({c[3]} req) {c[0]:.2f}->{c[4]:.2f}s'
-                  for c in srv.chunk_log[-6:]))
-    # solo rate per grid class (one of the server's own slots, its launch tuned on a scratch copy)
-    rate = {}
-    for key, idle in srv.pool.items():
-        s = idle[0].solver
-        s._dev.autotune(3)
-        ms = s._dev.time_steps(20)
-        rate[key] = s.info['nCells'] * 20 / (ms / 1e3)
-    lat_ser, mk_ser = SV.fifo_serial(reqs, lambda r: r.steps * r.cells / rate[(r.dx, r.heightM)])
+    log(f'[rank {rank}] served {stats["requests"]} requests in {stats["makespan_s"]:.1f} s: {stats["glups"]:.2f} GLUPS, '
+        f'p50 {stats["latency_p50_s"]:.2f} s, p99 {stats["latency_p99_s"]:.2f} s, {stats["chunks"]} chunks, '
+        f'host image building {stats["host_image_s"]:.1f} s')
+    srv.close()
+    # the serial arm: the same trace, each request alone, launch shapes tuned per class first
+    from ashburn_heat_twin_b200 import solver as S
+    shapes = {}
+    for r in reqs:
+        key = (r.dx, r.heightM)
+        if key not in shapes:
+            s = S.create_live_solver(backend=backend, static=st, dx=r.dx, allowAnyDx=True, heightM=r.heightM, u10Max=8,
+                                     met=r.met, existingFlux=r.flux)
+            by, zs, _ = s._dev.autotune(3)
+            shapes[key] = (by, zs)
+            s.step(64).result()
+            s.destroy()
+    sreqs = SV.requests_from_trace(trace, sim_s=SC.SERVE_SIM_S)
+    lat_ser, mk_ser, upd_ser = serve_serial(st, sreqs, backend, shapes)
+    mk_ser_all = RP.max_over_ranks(mk_ser, dist, f'cuda:{local}')
+    serial_glups = RP.aggregate_rate(upd_ser, world, mk_ser_all) / 1e9
+    log(f'[rank {rank}] serial: {len(sreqs)} requests in {mk_ser:.1f} s: {upd_ser / mk_ser / 1e9:.2f} GLUPS, '
+        f'p50 {np.percentile(lat_ser, 50):.2f} s, p99 {np.percentile(lat_ser, 99):.2f} s')
     upd = stats['cell_updates']
     h2d = sum(64 + 16 * int(round(r.heightM / r.dx)) + 20 * (6000 // int(r.dx)) ** 2 for r in reqs)
     d2h = sum((3 * 4 + min(int(round(r.heightM / r.dx)), int(round(420 / r.dx)))) * (6000 // int(r.dx)) ** 2
               for r in reqs)
     steps_total = sum(r.steps for r in reqs)
-    classes = {f'{int(k[0])} m': dict(solo_glups=v / 1e9) for k, v in rate.items()}
-    srv.close()
     out = dict(metric='GLUPS (all cells) served with continuous batching, Poisson trace of live-solver requests',
-               value=job_glups, unit='GLUPS', n_gpus=world, steps=stats['batch_steps'], warmup=6,
+               value=job_glups, unit='GLUPS', n_gpus=world, steps=stats['batch_steps'], warmup=len(warm),
                ms_per_step=stats['makespan_s'] * 1e3 / max(1, stats['batch_steps']), higher_is_better=True,
-               scaling='weak', vs_baseline=None,
-               dtype=DTYPE[a.precision],
+               scaling='weak', vs_baseline=None, dtype=DTYPE[a.precision],
                data='synthetic (seeded terrain, buildings and request trace; no public dataset involved)',
                config=dict(workload=WORKLOADS['c5']['desc'], requests=a.requests, rate_hz=a.rate, seed=a.seed,
-                           precision=a.precision, arith=a.arith, max_cells=a.max_cells, chunk=a.chunk,
-                           hbm_budget_bytes=srv.hbm_budget, batch_launch=srv.batch_launch,
-                           parallelism=f'replicas x{world}', classes=classes,
+                           precision=a.precision, scheme='pull', parallelism='replicas',
                            l2='per-step state of the admitted requests >> 126 MB L2'),
+               arith=a.arith, max_cells=a.max_cells, chunk=a.chunk, hbm_budget_bytes=srv.hbm_budget,
+               batch_mode=a.batch_mode,
                serving=dict(latency_p50_s=stats['latency_p50_s'], latency_p99_s=stats['latency_p99_s'],
                             latency_mean_s=stats['latency_mean_s'], queue_p50_s=stats['queue_p50_s'],
                             queue_p99_s=stats['queue_p99_s'], makespan_s=stats['makespan_s'],
-                            cell_updates=upd, chunks=stats['chunks'], batch_updates=stats['batch_rebuilds'],
-                            slots=stats['slots']),
-               serial=dict(value=upd / mk_ser / 1e9, unit='GLUPS', latency_p50_s=float(np.percentile(lat_ser, 50)),
+                            cell_updates=upd, chunks=stats['chunks'], slots=stats['slots'],
+                            host_image_s=stats['host_image_s'], server='ahx_server_* (C ABI scheduler thread)'),
+               serial=dict(value=serial_glups, unit='GLUPS', latency_p50_s=float(np.percentile(lat_ser, 50)),
                            latency_p99_s=float(np.percentile(lat_ser, 99)), makespan_s=mk_ser,
-                           what='the same trace solved back to back in arrival order, each request alone at its '
-                                'class solo device rate (host work not counted)'),
+                           cell_updates=upd_ser,
+                           what='the same trace run for real: each request alone through the public solver API '
+                                '(setMet, setExistingFlux, setNewCampuses, resetFlow, step, read) back to back in '
+                                'arrival order, set-up and read-back inside the wall clock'),
+               served_over_serial=job_glups / serial_glups if serial_glups > 0 else None,
                roofline=None, cpu_baseline=None,
                e2e=dict(value=job_glups, unit='GLUPS', h2d_bytes_per_step=h2d / steps_total,
                         d2h_bytes_per_step=d2h / steps_total,
-                        what='the served rate is end to end: request set-up uploads, batched steps and read() '
+                        what='the served rate is end to end: request images, uploads, batched steps and read() '
                              'downloads are all inside the wall-clock makespan'),
                gpu_launches=stats['batch_steps'], clocks=clocks)
     if dist is not None:
@@ -630,14 +657,12 @@ def main():
                          'Ashburn planes at its published grids), c3 (storage precision study), c4 (64 domains in one '
                          'batch), c5 (serving)')
     ap.add_argument('--members', type=int, default=64, help='batch: scenarios in the batch (64 = the full set)')
-    ap.add_argument('--requests', type=int, default=48, help='serving: requests in the trace')
+    ap.add_argument('--requests', type=int, default=500, help='serving: requests in the trace')
     ap.add_argument('--rate', type=float, default=50.0, help='serving: mean arrival rate (requests/s)')
     ap.add_argument('--seed', type=int, default=5, help='serving: trace seed')
     ap.add_argument('--max-cells', type=int, default=24_000_000,
                     help='serving: resident cell budget (24 M: the served rate of 64 M at a lower p50)')
-    ap.add_argument('--chunk', type=int, default=64, help='serving: steps per batched chunk')
-    ap.add_argument('--batch-minb', type=int, default=0, help='serving: batch register variant (4 / 5 / 6; 0 = default)')
-    ap.add_argument('--batch-zslab', type=int, default=0, help='serving: batch tile depth in levels (0 = default)')
+    ap.add_argument('--chunk', type=int, default=256, help='serving: steps per batched chunk')
     ap.add_argument('--batch-mode', default='branches', choices=['persistent', 'branches'],
                     help='serving: one persistent launch over tiles, or each request\'s own tuned kernel on parallel '
                          'graph branches')

@@ -282,6 +282,76 @@ ahx_status ahx_batch_set_launch(ahx_batch* b, int minb, int zslab, int use_graph
 ahx_status ahx_batch_get_info(ahx_batch* b, ahx_batch_info_out* out);
 ahx_status ahx_batch_destroy(ahx_batch* b);   /* idempotent; members are released */
 
+/* --- serving: continuous batching behind the C ABI -------------------------------------------------------------- */
+
+/* No counterpart in the reference: the live page serves one scenario at a time (js/live.js:69-86 steps it and reads
+ * it back in a loop). A server runs many scenario solves ("requests") on one device. The host builds each request's
+ * byte images exactly as for ahx_set_params / ahx_set_columns / ahx_set_ktop (the scenario's setMet,
+ * setExistingFlux and setNewCampuses, solver.js:225-376) and submits them with a step count and the read-back
+ * settings of ahx_read_submit. A scheduler thread inside the library admits requests in arrival order while the
+ * resident cells stay under max_cells and the slots' device memory under the HBM budget; it configures a solver slot
+ * (recycled from finished requests of the same grid, or created) as resetFlow would (equilibrium flow, theta 0, parity
+ * 0), steps every active request together in chunks of at most `chunk` steps with the batched launch (ahx_batch_*:
+ * each slot's own tuned step kernel on parallel graph branches, or one persistent launch), never past any request's
+ * step count, changes the member list between chunks (requests join and leave while others run: continuous
+ * batching), and answers a finished request with the read-back of its final state. Each answer is bit-identical to
+ * the same scenario stepped alone on a fresh handle. Host buffers are copied at submit and copied out at poll; the
+ * server owns all device memory. All calls are thread-safe. */
+typedef struct ahx_server ahx_server;
+
+typedef struct {
+  int32_t device_ordinal;    /* CUDA device; -1 = current */
+  int32_t precision, arith;  /* ahx_precision / ahx_arith of every slot */
+  int32_t chunk;             /* steps per batched chunk (<= 0: 256) */
+  int64_t max_cells;         /* resident-cell budget (<= 0: 24,000,000) */
+  uint64_t hbm_budget_bytes; /* device memory the slots may hold (0: 80 % of the memory free at creation) */
+  int32_t batch_mode;        /* 0: each slot's own step kernel on parallel graph branches; 1: one persistent launch */
+  int32_t tune;              /* 1: tune the launch shape on the first slot of each grid (ahx_autotune), reuse it */
+  int32_t depth;             /* chunks queued ahead of the scheduler (<= 0: 2) */
+  int32_t pad;
+} ahx_server_config;
+
+typedef struct {
+  int32_t nx, ny, nz;        /* grid of the scenario */
+  int32_t steps;             /* steps to run (>= 0) */
+  const void* params;        /* parameter block, params_bytes == 64 + 16 nz */
+  size_t params_bytes;
+  const uint32_t* colv;      /* 4 * nx * ny column records */
+  const uint32_t* ktop;      /* nx * ny ktop plane */
+  float conv, volscale;      /* read-back scaling, as ahx_read_submit */
+  int32_t nzv, want_vol, want_wind;
+  int32_t pad;
+  uint64_t user_tag;         /* returned in ahx_server_result */
+} ahx_request;
+
+typedef struct {
+  uint64_t ticket, user_tag;
+  int32_t nx, ny, nz, nzv, steps, status;    /* status: AHX_OK, or the error that ended the request */
+  double submitted_s, admitted_s, done_s;    /* seconds since the server was created */
+  float theta_max;                            /* unclamped max theta of the read-back levels */
+  int32_t want_vol, want_wind, pad;
+} ahx_server_result;
+
+typedef struct {
+  int64_t submitted, admitted, completed, queued, active;
+  int64_t cell_updates;      /* nx * ny * nz * steps summed over the chunks launched */
+  int64_t chunks, batch_steps, slots, idle_slots, evictions, resident_cells;
+  uint64_t slot_bytes, hbm_budget_bytes;
+  double elapsed_s;          /* since creation */
+} ahx_server_stats_out;
+
+ahx_status ahx_server_create(const ahx_server_config* cfg, ahx_server** out);
+/* copy the request in and queue it; returns its ticket at once */
+ahx_status ahx_server_submit(ahx_server* s, const ahx_request* req, uint64_t* ticket);
+/* wait up to timeout_ms (< 0: no bound) for the request; when it is done, fill *info and copy its read-back out
+ * (surf, u, v: nx * ny f32 north-up, u / v only with want_wind, vol: nzv * nx * ny u8 with want_vol; any may be NULL)
+ * and release the ticket. AHX_ETIMEOUT: not finished yet (the ticket stays valid). Returns the request's status. */
+ahx_status ahx_server_poll(ahx_server* s, uint64_t ticket, int timeout_ms, ahx_server_result* info, float* surf,
+                           float* u, float* v, uint8_t* vol);
+ahx_status ahx_server_stats(ahx_server* s, ahx_server_stats_out* out);
+/* stop the scheduler (requests not answered yet are dropped), release every slot and the batch; idempotent */
+ahx_status ahx_server_destroy(ahx_server* s);
+
 #ifdef __cplusplus
 }
 #endif

@@ -51,7 +51,7 @@ def test_serving_answers_match_solo_runs(st):
         r.sim_s = fresh(st, r).info['dt'] * (3 if r.dx == 40 else 5)
     c40 = fresh(st, reqs[0]).info['nCells']
     # cell budget of two 40 m grids: later requests queue and slots are recycled
-    srv = SV.Server(st, backend=oracle_backend(), batch_factory=SV.SequentialBatch, max_cells=2 * c40, chunk=2)
+    srv = SV.HostServer(st, backend=oracle_backend(), batch_factory=SV.SequentialBatch, max_cells=2 * c40, chunk=2)
     stats = srv.run(reqs, timeout_s=120)
     assert stats['requests'] == 5 and all(r.result is not None for r in reqs)
     assert [r.steps for r in reqs] == [3, 5, 3, 5, 3]
@@ -74,7 +74,7 @@ def test_serving_evicts_idle_slots_under_a_memory_budget(st):
         r.sim_s = 1e-6                               # one step each
     c20 = fresh(st, reqs[1]).info['nCells']
     budget = c20 * 208                               # one resident slot at a time: classes alternate, so evict
-    srv = SV.Server(st, backend=oracle_backend(), batch_factory=SV.SequentialBatch, max_cells=10**9,
+    srv = SV.HostServer(st, backend=oracle_backend(), batch_factory=SV.SequentialBatch, max_cells=10**9,
                     hbm_budget_bytes=budget)
     stats = srv.run(reqs, timeout_s=120)
     assert stats['requests'] == 4 and all(r.result is not None for r in reqs)
