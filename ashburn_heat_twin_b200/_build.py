@@ -11,6 +11,8 @@ Translation units and their arithmetic flags:
   batch.cu                    batched stepping (ahx_batch_*: tile tables, CUDA graph, stream ordering)
   noalloc.cu                  diagnostics over caller-owned buffers without allocation
   server.cu                   the serving scheduler thread (ahx_server_*: admission, batched chunks, read-back)
+  domain.cu      -fmad=false  the domain builder (ahx_static_*, ahx_domain_build: decode, aggregate, campus raster,
+                              build rules, column records)
 All use -ftz=true (f32 subnormals flushed, as the CPU restatement does); all but the fast variant use IEEE division
 and square root.
 """
@@ -45,6 +47,7 @@ UNITS = [(f'step_{v}_p{p}', 'step_unit.cu', flags + [f'-DAHX_STEP_PREC={p}'])
     ('noalloc', 'noalloc.cu', ['-fmad=false'] + IEEE),
     ('batch', 'batch.cu', ['-fmad=false'] + IEEE),
     ('server', 'server.cu', ['-fmad=false'] + IEEE),
+    ('domain', 'domain.cu', ['-fmad=false'] + IEEE),
 ]
 
 

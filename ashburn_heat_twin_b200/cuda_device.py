@@ -28,7 +28,8 @@ SYMBOLS = ('ahx_create', 'ahx_destroy', 'ahx_last_error', 'ahx_get_info', 'ahx_s
            'ahx_batch_create', 'ahx_batch_step', 'ahx_batch_time_steps', 'ahx_batch_sync', 'ahx_batch_set_launch',
            'ahx_batch_get_info', 'ahx_batch_destroy', 'ahx_batch_set_members', 'ahx_accum_enable', 'ahx_accum_read',
            'ahx_set_slab', 'ahx_row_bytes', 'ahx_row_pack', 'ahx_row_unpack', 'ahx_server_create',
-           'ahx_server_submit', 'ahx_server_poll', 'ahx_server_stats', 'ahx_server_destroy')
+           'ahx_server_submit', 'ahx_server_poll', 'ahx_server_stats', 'ahx_server_destroy', 'ahx_static_create',
+           'ahx_static_checksums', 'ahx_static_destroy', 'ahx_domain_build')
 
 
 class AhxError(RuntimeError):
@@ -83,6 +84,18 @@ class ServerStats(ctypes.Structure):
                                                'cell_updates', 'chunks', 'batch_steps', 'slots', 'idle_slots',
                                                'evictions', 'resident_cells')] + \
         [('slot_bytes', ctypes.c_uint64), ('hbm_budget_bytes', ctypes.c_uint64), ('elapsed_s', ctypes.c_double)]
+
+
+class DomainSpec(ctypes.Structure):
+    _fields_ = [('dx', ctypes.c_double), ('heightM', ctypes.c_double), ('extra_height', ctypes.c_double),
+                ('nz_min', ctypes.c_int32), ('ncampus', ctypes.c_int32), ('campus_mw', ctypes.c_void_p),
+                ('hall_count', ctypes.c_void_p), ('halls', ctypes.c_void_p), ('campus_flux', ctypes.c_void_p),
+                ('flux_existing', ctypes.c_double), ('kq', ctypes.c_double), ('cd_table', ctypes.c_void_p)]
+
+
+class DomainOut(ctypes.Structure):
+    _fields_ = [('nx', ctypes.c_int32), ('ny', ctypes.c_int32), ('nz', ctypes.c_int32), ('ktop_max', ctypes.c_int32),
+                ('zbase', ctypes.c_double), ('nb_cells', ctypes.c_int64)]
 
 
 class BudgetOut(ctypes.Structure):
@@ -159,6 +172,10 @@ def load_library(path: str = LIB_PATH):
         'ahx_server_poll': [H, ctypes.c_uint64, i, ctypes.POINTER(ServerResult), vp, vp, vp, vp],
         'ahx_server_stats': [H, ctypes.POINTER(ServerStats)],
         'ahx_server_destroy': [H],
+        'ahx_static_create': [i, i, i, vp, ctypes.c_size_t, vp, ctypes.POINTER(H)],
+        'ahx_static_checksums': [H, vp],
+        'ahx_static_destroy': [H],
+        'ahx_domain_build': [H, ctypes.POINTER(DomainSpec), ctypes.POINTER(DomainOut), vp, vp, vp, vp],
     }
     for name, args in sig.items():
         fn = getattr(L, name)

@@ -282,6 +282,50 @@ ahx_status ahx_batch_set_launch(ahx_batch* b, int minb, int zslab, int use_graph
 ahx_status ahx_batch_get_info(ahx_batch* b, ahx_batch_info_out* out);
 ahx_status ahx_batch_destroy(ahx_batch* b);   /* idempotent; members are released */
 
+/* --- domain builder on the GPU --------------------------------------------------------------------------------- */
+
+/* The host's domain and column images (js/live/domain.js loadStatic10 :32-69, aggregate :89-118, rasterizeCampuses
+ * :124-160, buildDomain :166-190; the column record of solver.js:359-376) built by kernels instead: the 10 m static
+ * planes are uploaded and decoded once (the dem's row-wise int16 first differences summed per row), each grid spacing
+ * is block-aggregated once, and each request's campuses, building rule and column records take three small launches.
+ * Every result is bit-identical to the host restatement (double precision in the reference's operation order). */
+typedef struct ahx_static ahx_static;
+
+/* raw: the decompressed static10 payload; offsets: byte offsets of the planes dem (low-byte plane, then high-byte
+ * plane, nrows * ncols each), lc (u8), frac25 (u8), hmean (u16 little-endian), dca4 (u8), as static10.json lists them */
+ahx_status ahx_static_create(int device_ordinal, int nrows, int ncols, const uint8_t* raw, size_t raw_bytes,
+                             const size_t* offsets, ahx_static** out);
+/* integer sums of the decoded planes, for the reference's checksums: dem (cm), lc, frac25, hmean (cm), dca4 */
+ahx_status ahx_static_checksums(ahx_static* s, int64_t* sums);
+ahx_status ahx_static_destroy(ahx_static* s);   /* idempotent */
+
+typedef struct {
+  double dx;                 /* grid spacing (m): a multiple of 10 that divides the box */
+  double heightM;            /* domain height (m) */
+  double extra_height;       /* minimum building height where a campus adds roof area (m; the reference uses 14) */
+  int32_t nz_min;            /* lower bound of nz (0: none) */
+  int32_t ncampus;           /* campuses, in list order */
+  const double* campus_mw;   /* heat load of each campus (MW) */
+  const int32_t* hall_count; /* halls of each campus */
+  const double* halls;       /* sum of hall_count entries of [x0, z0, x1, z1] (scene metres) */
+  double* campus_flux;       /* out: W per m^2 of each campus's total hall roof */
+  double flux_existing;      /* W per m^2 of operational data-center roof */
+  double kq;                 /* dt / (rho cp dx^3): K per step per W in one cell */
+  const double* cd_table;    /* 256 drag coefficients by land-cover class: (kappa / ln(0.5 dx / z0))^2 */
+} ahx_domain_spec;
+
+typedef struct {
+  int32_t nx, ny, nz, ktop_max;
+  double zbase;              /* floor(min dem) - dx (m) */
+  int64_t nb_cells;          /* building cells (sum of nb) */
+} ahx_domain_out;
+
+/* build one request's geometry: colv (4 * NXY u32: kt, ktop, cd f32 bits, q f32 bits) and ktop (NXY) in solver
+ * orientation (row 0 south), and the north-up campus heat (W) and new roof area (m^2) per cell; any output may be
+ * NULL. Synchronous. */
+ahx_status ahx_domain_build(ahx_static* s, const ahx_domain_spec* spec, ahx_domain_out* out, uint32_t* colv,
+                            uint32_t* ktop, double* heat_w, double* new_area);
+
 /* --- serving: continuous batching behind the C ABI -------------------------------------------------------------- */
 
 /* No counterpart in the reference: the live page serves one scenario at a time (js/live.js:69-86 steps it and reads

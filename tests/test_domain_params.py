@@ -121,3 +121,18 @@ def test_wind_profile_and_kprofile():
     assert PM.inflow_faces(210) == dict(w=1, e=0, s=1, n=0)
     assert PM.inflow_faces(75) == dict(w=0, e=1, s=0, n=1)
     assert PM.inflow_faces(180) == dict(w=0, e=0, s=1, n=0)
+
+
+def test_raw_payload_encoding_reproduces_static10(st):
+    """The payload the GPU domain builder uploads (gpu_domain.raw_payload) is, for the reference's own planes, byte for
+    byte the static10 payload: the dem as row-wise int16 first differences in low / high byte planes, then lc,
+    frac25, hmean (u16), dca4 at the offsets static10.json lists."""
+    import gzip
+    import os
+
+    from ashburn_heat_twin_b200 import gpu_domain as GD
+    raw, offs = GD.raw_payload(st)
+    ref = gzip.decompress(open(os.path.join(GOLDEN, 'static10.bin.gz'), 'rb').read())
+    P = st.meta['planes']
+    assert offs == [P[k]['offset'] for k in ('dem', 'lc', 'frac25', 'hmean', 'dca4')]
+    assert raw == ref[:len(raw)]
