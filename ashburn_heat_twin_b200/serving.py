@@ -31,6 +31,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
+from . import domain as D
 from . import solver as S
 
 
@@ -421,7 +422,7 @@ class NativeServer:
 
     def __init__(self, static, precision='fp32', arith='fast', device=None, max_cells=24_000_000, chunk=256,
                  hbm_budget_bytes=None, batch_mode='branches', tune=True, depth=2, u10Max=8.0, volMax=3.0,
-                 clock=time.perf_counter, sleep=time.sleep):
+                 gpu_domain=True, clock=time.perf_counter, sleep=time.sleep):
         from .cuda_device import Server as CServer
         self.static = static
         self.u10Max = u10Max
@@ -434,6 +435,12 @@ class NativeServer:
         self.max_cells, self.chunk = int(max_cells), int(chunk)
         self.hbm_budget = self.srv.stats()['hbm_budget_bytes']
         self.host_s = 0.0              # host time spent building images
+        # per-request geometry (campus raster, building rule, column records) by the GPU domain builder; the
+        # parameter block (met) stays on the host
+        self.gdom = None
+        if gpu_domain:
+            from .gpu_domain import GpuDomain
+            self.gdom = GpuDomain(static, device=device)
 
     def images(self, r: Request):
         """The byte images and read-back settings a fresh solver configured for r would use."""
@@ -443,15 +450,25 @@ class NativeServer:
             s = S.create_live_solver(backend=ImageRecorder, static=self.static, dx=r.dx, allowAnyDx=True,
                                      heightM=r.heightM, u10Max=self.u10Max, met=r.met, existingFlux=r.flux)
             self.templates[key] = s
+        dt = s.info['dt']
+        nx, ny, nz = s.info['nx'], s.info['ny'], s.info['nz']
         s.setMet(r.met)
+        rec = s._dev
+        if self.gdom is not None:
+            g = self.gdom.build(r.dx, heightM=r.heightM, campuses=[r.campus], flux=r.flux, dt=dt, nzMin=nz)
+            if g['nz'] == nz:
+                # heat of the request: the sequential sum over solver rows of existing + campus W (solver.js:359-376)
+                Wn = s._agg.dcarea * float(r.flux) + g['heatW']
+                totalW = float(np.cumsum(D.flip_rows(Wn, nx, ny))[-1])
+                return dict(nx=nx, ny=ny, nz=nz, params=rec.params, colv=g['colv'], ktop=g['ktop'],
+                            conv=np.float32(s._conv), volscale=np.float32(255 / self.volMax), nzv=s.nzv, dt=dt,
+                            heatMW=totalW / 1e6, steps=int(math.ceil(r.sim_s / dt - 1e-9)))
         s.setExistingFlux(r.flux)
         s.setNewCampuses([r.campus])
         s.resetFlow()
-        rec = s._dev
-        dt = s.info['dt']
-        return dict(nx=s.info['nx'], ny=s.info['ny'], nz=s.info['nz'], params=rec.params, colv=rec.colv,
-                    ktop=rec.ktop, conv=np.float32(s._conv), volscale=np.float32(255 / self.volMax), nzv=s.nzv, dt=dt,
-                    heatMW=s._heatMW, steps=int(math.ceil(r.sim_s / dt - 1e-9)))
+        return dict(nx=nx, ny=ny, nz=nz, params=rec.params, colv=rec.colv, ktop=rec.ktop, conv=np.float32(s._conv),
+                    volscale=np.float32(255 / self.volMax), nzv=s.nzv, dt=dt, heatMW=s._heatMW,
+                    steps=int(math.ceil(r.sim_s / dt - 1e-9)))
 
     def submit(self, r: Request):
         t = self.clock()
@@ -532,6 +549,9 @@ class NativeServer:
         for s in self.templates.values():
             s.destroy()
         self.templates = {}
+        if self.gdom is not None:
+            self.gdom.destroy()
+            self.gdom = None
         self.srv.destroy()
 
 

@@ -82,3 +82,19 @@ def test_server_recycles_slots_and_handles_zero_step_requests():
         assert np.array_equal(r.result['surf'], ref['surf']) and r.result['steps'] == r.steps
     assert reqs[0].steps == 0
     srv.close()
+
+
+def test_gpu_built_request_images_equal_the_host_images():
+    """The serving loop builds each request's geometry with the GPU domain builder: its column records, ktop plane and
+    heat equal what a solver configured on the host uploads, for every grid class of the mix."""
+    st = small_static(seed=9, ncols=120, nrows=96)
+    reqs = _requests(st, n=6, seed=5)
+    g = SV.NativeServer(st, precision='fp32', arith='fast', tune=False)
+    h = SV.NativeServer(st, precision='fp32', arith='fast', tune=False, gpu_domain=False)
+    for r in reqs:
+        a, b = g.images(r), h.images(r)
+        assert a['params'] == b['params'] and (a['nx'], a['ny'], a['nz']) == (b['nx'], b['ny'], b['nz'])
+        assert np.array_equal(np.asarray(a['colv']).ravel(), np.asarray(b['colv']).ravel())
+        assert np.array_equal(a['ktop'], b['ktop']) and a['heatMW'] == b['heatMW'] and a['steps'] == b['steps']
+    g.close()
+    h.close()
