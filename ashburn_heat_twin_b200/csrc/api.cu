@@ -87,6 +87,7 @@ DomainView ahx::view_at(ahx_handle* h, int parity) {
   D.nyg = slab ? h->nyg : h->dims.ny;
   D.jlo = slab ? h->jlo : 0;
   D.jhi = slab ? h->jhi : h->dims.ny;
+  D.jbase = 0;
   D.ps = h->ps;
   D.qs = h->qs;
   set_offsets(D);
@@ -957,6 +958,63 @@ static ahx_status row_copy(ahx_handle* h, int j, void* buf, int to_buffer) {
 ahx_status ahx_row_pack(ahx_handle* h, int j, void* dst_device) { return row_copy(h, j, dst_device, 1); }
 ahx_status ahx_row_unpack(ahx_handle* h, int j, const void* src_device) {
   return row_copy(h, j, const_cast<void*>(src_device), 0);
+}
+
+ahx_status ahx_halo_bytes(ahx_handle* h, size_t* bytes) {
+  if (!h || !bytes) return fail(AHX_EINVAL, "live solver: null argument");
+  std::lock_guard<std::mutex> lk(h->mu);
+  if (ahx_status st = check(h)) return st;
+  const size_t per = (size_t)h->dims.nz * h->dims.nx;
+  *bytes = ((5 * per * h->esize + 15) & ~(size_t)15) + per * h->esize_g;   // f part padded to 16 bytes
+  return AHX_OK;
+}
+
+static ahx_status halo_copy(ahx_handle* h, int j, int dir, int next, void* buf, int to_buffer) {
+  if (!h || !buf) return fail(AHX_EINVAL, "live solver: null argument");
+  if (dir != 1 && dir != -1) return fail(AHX_EINVAL, "live solver: halo direction must be +1 or -1");
+  if ((reinterpret_cast<uintptr_t>(buf) & 15) != 0) return fail(AHX_EINVAL, "live solver: halo buffer not 16-byte aligned");
+  std::lock_guard<std::mutex> lk(h->mu);
+  if (ahx_status st = check(h)) return st;
+  if (j < 0 || j >= h->dims.ny) return fail(AHX_EINVAL, "live solver: row out of range");
+  AHX_CUDA(h, cudaSetDevice(h->dev));
+  const DomainView D = view(h);
+  AHX_CUDA(h, launch_halo_copy(D, h->dims.precision, j, dir, next, buf, to_buffer, h->s_step));
+  return AHX_OK;
+}
+
+ahx_status ahx_halo_pack(ahx_handle* h, int j, int dir, int next, void* dst_device) {
+  return halo_copy(h, j, dir, next ? 1 : 0, dst_device, 1);
+}
+ahx_status ahx_halo_unpack(ahx_handle* h, int j, int dir, const void* src_device) {
+  return halo_copy(h, j, dir, 0, const_cast<void*>(src_device), 0);
+}
+
+ahx_status ahx_step_rows(ahx_handle* h, int j0, int j1, int advance) {
+  if (!h) return fail(AHX_EINVAL, "live solver: null handle");
+  std::lock_guard<std::mutex> lk(h->mu);
+  if (ahx_status st = check(h)) return st;
+  const int lo = h->nyg > 0 ? h->jlo : 0, hi = h->nyg > 0 ? h->jhi : h->dims.ny;
+  if (j0 < lo || j1 > hi || j0 > j1) return fail(AHX_EINVAL, "live solver: rows outside the updated range");
+  if (h->dims.precision == AHX_FP16_SR)
+    return fail(AHX_EINVAL, "live solver: a stochastic-rounding state steps whole (its dithers count the step's blocks)");
+  if (h->budget_on || h->accum_on)
+    return fail(AHX_EINVAL, "live solver: budgets and accumulators are taken over whole steps");
+  AHX_CUDA(h, cudaSetDevice(h->dev));
+  if (j1 > j0) {
+    StepLaunch L = solo_launch(h, h->parity);
+    L.tma_ty = 0;
+    L.maps = nullptr;
+    DomainView D = view(h);
+    D.jlo = j0;
+    D.jhi = j1;
+    D.jbase = j0;
+    AHX_CUDA(h, h->dims.arith == AHX_ARITH_FAST ? fast::launch_step(D, L, h->s_step) : exact::launch_step(D, L, h->s_step));
+  }
+  if (advance) {
+    h->parity ^= 1;
+    ++h->steps;
+  }
+  return AHX_OK;
 }
 
 ahx_status ahx_set_launch(ahx_handle* h, int block_y, int zslab) {

@@ -330,6 +330,48 @@ __global__ void __launch_bounds__(256) row_copy_kernel(DomainView D, int j, cons
   }
 }
 
+// The halo of a y-slab boundary: of row j, only the populations that cross the boundary toward the neighbour, c_y =
+// dir (+1: the 5 flow populations and 1 temperature population moving north, which the north neighbour's first row
+// pulls from its ghost row; -1: those moving south). Packed as [5][nz][nx] f, padded to 16 bytes, then [nz][nx] g.
+// `src` selects the buffers (the state a step reads, or the one the step in progress writes).
+struct HaloPlanes {
+  int f[5], g;
+};
+__host__ __device__ constexpr HaloPlanes halo_planes(int dir) {
+  HaloPlanes h{{0, 0, 0, 0, 0}, 0};
+  int n = 0;
+  for (int q = 0; q < 19; ++q)
+    if (kC19[q][1] == dir) h.f[n++] = q;
+  for (int q = 0; q < 7; ++q)
+    if (kC7[q][1] == dir) h.g = q;
+  return h;
+}
+static_assert(halo_planes(1).f[4] != 0 && halo_planes(-1).f[4] != 0, "five flow populations cross each boundary");
+
+template <class TF, class TG, int DIR>
+__global__ void __launch_bounds__(256) halo_copy_kernel(DomainView D, int j, const void* f, const void* g, void* buf,
+                                                        int to_buffer) {
+  const long per = (long)D.nz * D.nx;
+  const long e = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= 6 * per) return;
+  const int slot = (int)(e / per);
+  const int k = (int)((e % per) / D.nx), i = (int)(e % D.nx);
+  const uint32_t n = (uint32_t)k * D.ps + (uint32_t)j * (uint32_t)D.px + (uint32_t)i;
+  constexpr HaloPlanes H = halo_planes(DIR);
+  if (slot < 5) {
+    TF* s = const_cast<TF*>(static_cast<const TF*>(f)) + (uint32_t)H.f[slot] * D.qs + n;
+    TF* b = static_cast<TF*>(buf) + (long)slot * per + (long)k * D.nx + i;
+    if (to_buffer) *b = *s;
+    else *s = *b;
+  } else {
+    TG* s = const_cast<TG*>(static_cast<const TG*>(g)) + (uint32_t)H.g * D.qs + n;
+    const size_t goff = (5 * (size_t)per * sizeof(TF) + 15) & ~(size_t)15;
+    TG* b = reinterpret_cast<TG*>(static_cast<unsigned char*>(buf) + goff) + (long)k * D.nx + i;
+    if (to_buffer) *b = *s;
+    else *s = *b;
+  }
+}
+
 template <class F>
 cudaError_t dispatch(int precision, F&& f) {
   switch (precision) {
@@ -421,6 +463,20 @@ cudaError_t launch_export_plane(const DomainView& D, int precision, const void* 
     else
       export_plane_kernel<StoreF<S>><<<grid, 256, 0, s>>>(D, static_cast<const StoreF<S>*>(src), ref_plane,
                                                           ref_is_f64, q, 0);
+    return cudaGetLastError();
+  });
+}
+
+cudaError_t launch_halo_copy(const DomainView& D, int precision, int j, int dir, int next, void* buf, int to_buffer,
+                             cudaStream_t s) {
+  return dispatch(precision, [&](auto tag) {
+    using S = decltype(tag);
+    const long total = 6L * D.nz * D.nx;
+    const unsigned blocks = (unsigned)((total + 255) / 256);
+    const void* f = next ? D.fB : D.fA;
+    const void* g = next ? D.gB : D.gA;
+    if (dir > 0) halo_copy_kernel<StoreF<S>, StoreG<S>, 1><<<blocks, 256, 0, s>>>(D, j, f, g, buf, to_buffer);
+    else halo_copy_kernel<StoreF<S>, StoreG<S>, -1><<<blocks, 256, 0, s>>>(D, j, f, g, buf, to_buffer);
     return cudaGetLastError();
   });
 }

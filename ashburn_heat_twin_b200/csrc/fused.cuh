@@ -682,7 +682,7 @@ __device__ __forceinline__ void step_block(const DomainView& D, int bx, int by, 
   const RelaxConst RK = relax_const(P);
 
   const int i = bx * kBlockX + threadIdx.x;
-  const int j = by * blockDim.y + threadIdx.y;
+  const int j = D.jbase + by * (int)blockDim.y + (int)threadIdx.y;
   const int k0 = bz * zslab;
   const int k1 = min(D.nz, k0 + zslab);
   BudgetAcc B;

@@ -302,6 +302,7 @@ struct DomainView {
   // y-slab of a larger domain: local row 0 is global row jg0 of nyg; only local rows [jlo, jhi) are updated (the
   // others are ghost rows refreshed from the neighbouring slabs); a whole domain has jg0 0, nyg ny, [0, ny)
   int jg0, nyg, jlo, jhi;
+  int jbase;                    // first local row the launch's grid covers (0 unless a step of a band of rows)
   uint32_t ps;                  // plane stride px*ny
   uint32_t qs;                  // q stride px*ny*nz
   // element offset of the interior pull source of population q relative to the cell: q*qs - (cx + cy*px + cz*ps)

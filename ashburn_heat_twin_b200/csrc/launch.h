@@ -80,6 +80,10 @@ cudaError_t launch_export_plane(const DomainView& D, int precision, const void* 
 
 // copy local row j of all 26 planes of the current state (D.fA / D.gA) to (to_buffer) or from a packed device buffer
 cudaError_t launch_row_copy(const DomainView& D, int precision, int j, void* buf, int to_buffer, cudaStream_t s);
+// copy the halo of local row j (the 6 planes with c_y = dir) of the current state (next = 0: D.fA / D.gA) or of the
+// state the step in progress writes (next = 1: D.fB / D.gB) to (to_buffer) or from a packed device buffer
+cudaError_t launch_halo_copy(const DomainView& D, int precision, int j, int dir, int next, void* buf, int to_buffer,
+                             cudaStream_t s);
 
 int element_bytes(int precision);     // bytes of one stored flow population f
 int element_bytes_g(int precision);   // bytes of one stored temperature population g

@@ -29,7 +29,8 @@ SYMBOLS = ('ahx_create', 'ahx_destroy', 'ahx_last_error', 'ahx_get_info', 'ahx_s
            'ahx_batch_get_info', 'ahx_batch_destroy', 'ahx_batch_set_members', 'ahx_accum_enable', 'ahx_accum_read',
            'ahx_set_slab', 'ahx_row_bytes', 'ahx_row_pack', 'ahx_row_unpack', 'ahx_server_create',
            'ahx_server_submit', 'ahx_server_poll', 'ahx_server_stats', 'ahx_server_destroy', 'ahx_static_create',
-           'ahx_static_checksums', 'ahx_static_destroy', 'ahx_domain_build')
+           'ahx_static_checksums', 'ahx_static_destroy', 'ahx_domain_build', 'ahx_halo_bytes', 'ahx_halo_pack',
+           'ahx_halo_unpack', 'ahx_step_rows')
 
 
 class AhxError(RuntimeError):
@@ -164,6 +165,10 @@ def load_library(path: str = LIB_PATH):
         'ahx_row_bytes': [H, ctypes.POINTER(ctypes.c_size_t)],
         'ahx_row_pack': [H, i, vp],
         'ahx_row_unpack': [H, i, vp],
+        'ahx_halo_bytes': [H, ctypes.POINTER(ctypes.c_size_t)],
+        'ahx_halo_pack': [H, i, i, i, vp],
+        'ahx_halo_unpack': [H, i, i, vp],
+        'ahx_step_rows': [H, i, i, i],
         'ahx_accum_read': [H, vp, vp, ctypes.POINTER(ctypes.c_int64), i],
         'ahx_batch_get_info': [H, ctypes.POINTER(BatchInfoOut)],
         'ahx_batch_destroy': [H],
@@ -414,6 +419,25 @@ class CudaDevice:
 
     def row_unpack(self, j, src_ptr):
         self._c('ahx_row_unpack', int(j), ctypes.c_void_p(int(src_ptr)))
+
+    def halo_bytes(self):
+        b = ctypes.c_size_t()
+        self._c('ahx_halo_bytes', ctypes.byref(b))
+        return b.value
+
+    def halo_pack(self, j, direction, dst_ptr, next_state=False):
+        """queue a copy of the halo of local row j (the 6 planes with c_y = direction) into device memory at dst_ptr,
+        from the current state or (next_state) from the one the step in progress writes"""
+        self._c('ahx_halo_pack', int(j), int(direction), int(bool(next_state)), ctypes.c_void_p(int(dst_ptr)))
+
+    def halo_unpack(self, j, direction, src_ptr):
+        self._c('ahx_halo_unpack', int(j), int(direction), ctypes.c_void_p(int(src_ptr)))
+
+    def step_rows(self, j0, j1, advance):
+        """one step restricted to local rows [j0, j1); the call with advance completes the step"""
+        self._c('ahx_step_rows', int(j0), int(j1), int(bool(advance)))
+        if advance:
+            self._p ^= 1
 
     def accum_enable(self, on=True):
         self._c('ahx_accum_enable', int(bool(on)))

@@ -3,11 +3,14 @@ one GPU's share (a 5 m grid, 1200x1200x128, needs ~100 GB in FP32).
 
 The host builds the whole domain once (the live solver's own domain and parameter code, on a recording device that
 only keeps the host images) and gives each slab its rows of the column records and the ktop plane, plus one ghost row
-on each internal boundary. Every step is: each slab steps its own rows (faces and sponges follow the global rows);
-then each slab's boundary rows are packed into device buffers and unpacked into the neighbours' ghost rows. On one
-device the copies stay on the device; across GPUs the packed rows go over NCCL (send / recv of 26 x nz x nx
-elements per boundary per step) with one process per slab. The stepped rows are bit-identical to the undivided
-domain's.
+on each internal boundary. A neighbour's first row pulls from its ghost row only the populations that move toward it
+(c_y = +1 northward, -1 southward: 5 flow and 1 temperature population), so each boundary exchanges a halo of 6 of the
+26 planes per direction (ahx_halo_*). Every step is split (ahx_step_rows): a slab updates its boundary rows first,
+packs their halos from the state being written, queues its interior rows, and only then waits for the packs, so the
+transfer (device copies on one GPU; NCCL send / recv of 6 x nz x nx elements per direction across GPUs, one process
+per slab) overlaps the interior update; the received halos are unpacked into the ghost rows behind the step. Faces and
+sponges follow the global rows, so the stepped rows are bit-identical to the undivided domain's. A stochastic-rounding
+state steps whole (its dithers count the step's blocks) and exchanges the same halos after the step.
 """
 from __future__ import annotations
 
@@ -91,33 +94,49 @@ class SlabDomain:
             d.clear_heat()
             self.slabs.append(dict(dev=d, a=a, b=b, jg0=jg0, ny=nyl, lo=ga, hi=ga + (b - a)))
         import torch
-        nb = (self.slabs[0]['dev'].row_bytes() + 255) // 256 * 256   # keep the second half 256-byte aligned
+        nb = (self.slabs[0]['dev'].halo_bytes() + 255) // 256 * 256   # keep the second half 256-byte aligned
         self._buf = [torch.empty(2 * nb, dtype=torch.uint8, device=f'cuda:{device or 0}')
                      for _ in range(len(self.slabs) - 1)]
         self._nb = nb
+        self.split = precision != 'fp16sr'
         self.steps = 0
 
-    def exchange(self):
-        """refresh every ghost row from the neighbouring slab's boundary row (device copies, in order)"""
-        for r in range(len(self.slabs) - 1):
-            lo, hi = self.slabs[r], self.slabs[r + 1]
-            buf = self._buf[r]
-            p0, p1 = buf.data_ptr(), buf.data_ptr() + self._nb
-            lo['dev'].row_pack(lo['hi'] - 1, p0)        # south slab's last owned row -> north slab's ghost row 0
-            hi['dev'].row_pack(hi['lo'], p1)            # north slab's first owned row -> south slab's top ghost row
-            lo['dev'].sync()
-            hi['dev'].sync()
-            hi['dev'].row_unpack(0, p0)
-            lo['dev'].row_unpack(lo['ny'] - 1, p1)
+    def step(self, n=1):
+        """n steps; after each, every ghost row holds the neighbour's new halo (device copies)"""
+        last = len(self.slabs) - 1
+        for _ in range(int(n)):
+            for r, s in enumerate(self.slabs):
+                dev, south, north = s['dev'], r > 0, r < last
+                bs = self._buf[r - 1].data_ptr() + self._nb if south else None   # my south-moving halo
+                bn = self._buf[r].data_ptr() if north else None                   # my north-moving halo
+                if self.split:
+                    a = s['lo'] + int(south)
+                    b = s['hi'] - int(north)
+                    if south:
+                        dev.step_rows(s['lo'], s['lo'] + 1, False)
+                    if north and s['hi'] - 1 >= a:
+                        dev.step_rows(s['hi'] - 1, s['hi'], False)
+                    if south:
+                        dev.halo_pack(s['lo'], -1, bs, next_state=True)
+                    if north:
+                        dev.halo_pack(s['hi'] - 1, 1, bn, next_state=True)
+                    dev.step_rows(a, max(a, b), True)
+                else:
+                    dev.step(1, 0)
+                    if south:
+                        dev.halo_pack(s['lo'], -1, bs)
+                    if north:
+                        dev.halo_pack(s['hi'] - 1, 1, bn)
+            for s in self.slabs:
+                s['dev'].sync()
+            for r in range(last):
+                lo, hi = self.slabs[r], self.slabs[r + 1]
+                p0, p1 = self._buf[r].data_ptr(), self._buf[r].data_ptr() + self._nb
+                hi['dev'].halo_unpack(0, 1, p0)                 # into the north slab's ghost row 0
+                lo['dev'].halo_unpack(lo['ny'] - 1, -1, p1)     # into the south slab's top ghost row
+            self.steps += 1
         for s in self.slabs:
             s['dev'].sync()
-
-    def step(self, n=1):
-        for _ in range(int(n)):
-            for s in self.slabs:
-                s['dev'].step(1, 0)
-            self.exchange()
-            self.steps += 1
 
     def read_state(self):
         """f (19, nz, ny, nx) and g (7, nz, ny, nx) of the whole domain, from the slabs' owned rows."""
@@ -168,23 +187,47 @@ class DistributedSlab:
         self.dev.set_ktop(np.ascontiguousarray(img.ktop[self.jg0:self.jg0 + self.nyl]).reshape(-1), None)
         self.dev.init_flow()
         self.dev.clear_heat()
-        nb = (self.dev.row_bytes() + 255) // 256 * 256
+        nb = (self.dev.halo_bytes() + 255) // 256 * 256
         dv = f'cuda:{device or 0}'
         self._nb = nb
+        self._dv = dv
         self._send = torch.empty(2 * nb, dtype=torch.uint8, device=dv)
         self._recv = torch.empty(2 * nb, dtype=torch.uint8, device=dv)
         self._host = dist.get_backend() != 'nccl'
+        self.split = precision != 'fp16sr'
         self.steps = 0
 
-    def exchange(self):
-        """ghost rows from the neighbouring ranks (every rank takes the same steps in the same order)"""
+    def _step_and_pack(self):
+        """this rank's part of one step up to the halos it sends: boundary rows, their halos from the state being
+        written, then the interior rows queued behind them; returns once the halos are in the send buffers"""
         south, north = self.rank > 0, self.rank < self.world - 1
         s0, s1 = self._send.data_ptr(), self._send.data_ptr() + self._nb
-        if south:
-            self.dev.row_pack(self.lo, s0)            # my first owned row -> the south neighbour's top ghost row
-        if north:
-            self.dev.row_pack(self.hi - 1, s1)        # my last owned row -> the north neighbour's ghost row 0
-        self.dev.sync()
+        if self.split:
+            a, b = self.lo + int(south), self.hi - int(north)
+            if south:
+                self.dev.step_rows(self.lo, self.lo + 1, False)
+            if north and self.hi - 1 >= a:
+                self.dev.step_rows(self.hi - 1, self.hi, False)
+            if south:
+                self.dev.halo_pack(self.lo, -1, s0, next_state=True)   # my first row's south-moving halo
+            if north:
+                self.dev.halo_pack(self.hi - 1, 1, s1, next_state=True)   # my last row's north-moving halo
+            packed = self.dev.fence()
+            self.dev.step_rows(a, max(a, b), True)                         # the interior overlaps the exchange
+            packed.result()
+        else:
+            self.dev.step(1, 0)
+            if south:
+                self.dev.halo_pack(self.lo, -1, s0)
+            if north:
+                self.dev.halo_pack(self.hi - 1, 1, s1)
+            self.dev.sync()
+
+    def exchange(self):
+        """send this rank's halos and unpack the neighbours' into the ghost rows (every rank takes the same steps in
+        the same order)"""
+        import torch
+        south, north = self.rank > 0, self.rank < self.world - 1
         nb = self._nb
         send = self._send.cpu() if self._host else self._send
         recv = self._recv.cpu() if self._host else self._recv
@@ -200,16 +243,18 @@ class DistributedSlab:
                 w.wait()
         if self._host:
             self._recv.copy_(recv)
+        # the received halos are in place once torch's stream (NCCL's waits, the host copy) has run
+        torch.cuda.current_stream(self._dv).synchronize()
         r0, r1 = self._recv.data_ptr(), self._recv.data_ptr() + nb
         if south:
-            self.dev.row_unpack(0, r0)
+            self.dev.halo_unpack(0, 1, r0)                  # the south neighbour's north-moving halo
         if north:
-            self.dev.row_unpack(self.nyl - 1, r1)
+            self.dev.halo_unpack(self.nyl - 1, -1, r1)      # the north neighbour's south-moving halo
         self.dev.sync()
 
     def step(self, n=1):
         for _ in range(int(n)):
-            self.dev.step(1, 0)
+            self._step_and_pack()
             self.exchange()
             self.steps += 1
 

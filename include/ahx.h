@@ -242,6 +242,20 @@ ahx_status ahx_set_slab(ahx_handle* h, int jg0, int nyg, int jlo, int jhi);
 ahx_status ahx_row_bytes(ahx_handle* h, size_t* bytes);
 ahx_status ahx_row_pack(ahx_handle* h, int j, void* dst_device);
 ahx_status ahx_row_unpack(ahx_handle* h, int j, const void* src_device);
+/* The halo of a boundary: of local row j, only the populations that cross to the neighbour, c_y = dir (+1: the 5 flow
+ * and 1 temperature populations moving north, which the north slab's first row pulls from its ghost row; -1: those
+ * moving south), 6 of the 26 planes. Packed as [5][nz][nx] f elements, padded to 16 bytes, then [nz][nx] g elements
+ * (ahx_halo_bytes); buffers 16-byte aligned. ahx_halo_pack reads the current state (next = 0) or the state the step in
+ * progress writes (next = 1, between ahx_step_rows calls of one step); ahx_halo_unpack writes the current state. */
+ahx_status ahx_halo_bytes(ahx_handle* h, size_t* bytes);
+ahx_status ahx_halo_pack(ahx_handle* h, int j, int dir, int next, void* dst_device);
+ahx_status ahx_halo_unpack(ahx_handle* h, int j, int dir, const void* src_device);
+/* One step in parts: update only local rows [j0, j1) (within the rows the handle updates) from the current state into
+ * the next one; the call with advance = 1 completes the step (the state read by later calls flips). A slab steps its
+ * boundary rows first, packs their halos (next = 1) for the neighbours, and then its interior rows, so the halo
+ * transfer overlaps the interior update. The parts of a step are bit-identical to one whole step. Not for
+ * AHX_FP16_SR storage or with budgets or accumulators enabled (AHX_EINVAL). */
+ahx_status ahx_step_rows(ahx_handle* h, int j0, int j1, int advance);
 
 /* --- batched stepping ----------------------------------------------------------------------------------------- */
 
