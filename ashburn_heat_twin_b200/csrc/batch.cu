@@ -277,6 +277,17 @@ ahx_status ensure_capacity(ahx_batch* b, int members, int64_t tiles, int nz) {
   return AHX_OK;
 }
 
+// tiles of a member domain in x and y (32 x 4 columns per tile): the main tiles, then the strip tiles of its column
+// split (a batch member is a whole domain)
+struct TileGrid {
+  int gx, gy;
+};
+TileGrid tile_grid(const ahx_handle* h) {
+  const int nx = h->dims.nx, ny = h->dims.ny;
+  const StepSplit SP = step_split(nx, 0, ny, 0, 0, ny, strip_width(h->esize));
+  return TileGrid{SP.gx, main_blocks_y(ny, 0, 4) + strip_blocks_y(SP, 4)};
+}
+
 // Tile plan for depth policy `policy` (> 0: that depth for every member, clipped to its nz, 8 levels by default;
 // -1: whole columns when that still gives at least 4 tiles per persistent block, else each member's own z-slab or
 // 16 levels).
@@ -286,7 +297,7 @@ ahx_status build_plan(const std::vector<ahx_handle*>& mem, int policy, int grid,
     return h->zslab > 0 ? std::min(h->zslab, h->dims.nz) : std::min(h->dims.nz, 16);
   };
   int64_t whole_tiles = 0;
-  for (const ahx_handle* h : mem) whole_tiles += (int64_t)((h->dims.nx + 31) / 32) * ((h->dims.ny + 3) / 4);
+  for (const ahx_handle* h : mem) whole_tiles += (int64_t)tile_grid(h).gx * tile_grid(h).gy;
   const bool whole = policy < 0 && whole_tiles >= 4 * (int64_t)std::max(grid, 1);
   tiles.clear();
   zslab.clear();
@@ -295,7 +306,8 @@ ahx_status build_plan(const std::vector<ahx_handle*>& mem, int policy, int grid,
     const int nz = h->dims.nz;
     const int zs = policy > 0 ? std::min(policy, nz) : (whole ? nz : own(h));
     zslab.push_back(zs);
-    const int gx = (h->dims.nx + 31) / 32, gy = (h->dims.ny + 3) / 4, gz = (nz + zs - 1) / zs;
+    const TileGrid tg = tile_grid(h);
+    const int gx = tg.gx, gy = tg.gy, gz = (nz + zs - 1) / zs;
     if (gx > 65535 || gy > 65535 || gz > 65535)
       return fail(AHX_EINVAL, "live solver: member grid too large for a batch tile index");
     if (tiles.size() + (size_t)gx * gy * gz > (size_t)INT32_MAX / 2)
@@ -319,7 +331,7 @@ ahx_status upload(ahx_batch* b, const std::vector<ahx_handle*>& mem, const std::
     g.views[m] = view_at(h, h->parity);
     g.views[C + m] = view_at(h, h->parity ^ 1);
     // tiles of this member in one step (its blocks report done to its step counter)
-    const uint32_t nt = (uint32_t)((h->dims.nx + 31) / 32) * (uint32_t)((h->dims.ny + 3) / 4) *
+    const uint32_t nt = (uint32_t)tile_grid(h).gx * (uint32_t)tile_grid(h).gy *
                         (uint32_t)((h->dims.nz + zslab[m] - 1) / zslab[m]);
     g.views[m].tick_blocks = g.views[C + m].tick_blocks = nt;
     g.zslab[m] = zslab[m];

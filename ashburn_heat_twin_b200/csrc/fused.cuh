@@ -177,6 +177,73 @@ __device__ __forceinline__ R feq_poly(R cu, R usq) {
   return nsub(nadd(nadd(R(1.0), nmul(R(3.0), cu)), nmul(nmul(R(4.5), cu), cu)), nmul(R(1.5), usq));
 }
 
+// The lateral-face rules of the stream for a cell of a face column (C.face), after its populations were loaded with
+// every outside source taken from the own cell: secOutflowPrelude (kernel.js:122-148) and the in/outflow cases of
+// secStreamF / secStreamG (kernel.js:187-204, 219-243). f and g are the decoded populations of cell n at level k (top:
+// k is the lid level). The formulas use non-contractible operations, so every kernel path gives the same bits.
+template <class S>
+__device__ __forceinline__ void face_patch(const DomainView& D, const ParamsHead& P, const Column<RealOf<S>>& C,
+                                           bool top, uint32_t n, RealOf<S> uI, RealOf<S> vI, RealOf<S> (&f)[19],
+                                           RealOf<S> (&g)[7]) {
+  using R = RealOf<S>;
+  using KF = CodecF<S>;
+  const StoreF<S>* fA = static_cast<const StoreF<S>*>(D.fA);
+  const uint32_t qs = D.qs;
+  // secOutflowPrelude (kernel.js:122-148): own-cell density and velocity on outflow faces
+  R rn = R(1), uxn = R(0), uyn = R(0), uzn = R(0);
+  if (C.onb) {
+    R own[19];
+    static_for<19>([&](auto Q) {
+      constexpr int q = Q;
+      own[q] = KF::dec_f(KF::load(fA + (uint32_t)q * qs + n), R(w19(q)));
+    });
+    rn = own[0];
+#pragma unroll
+    for (int q = 1; q < 19; ++q) rn = rn + own[q];
+    auto fo = [&](int q) { return own[q]; };
+    uxn = moment1<R, 0>(fo) / rn;
+    uyn = moment1<R, 1>(fo) / rn;
+    uzn = moment1<R, 2>(fo) / rn;
+  }
+  const R usqn = nadd(nadd(nmul(uxn, uxn), nmul(uyn, uyn)), nmul(uzn, uzn));
+  R uxc = uxn, uyc = uyn;
+  if (P.oclip != 0) {
+    if (C.latW && P.inflow_w == 0 && uxc > R(0)) uxc = R(0);
+    if (C.latE && P.inflow_e == 0 && uxc < R(0)) uxc = R(0);
+    if (C.latS && P.inflow_s == 0 && uyc > R(0)) uyc = R(0);
+    if (C.latN && P.inflow_n == 0 && uyc < R(0)) uyc = R(0);
+  }
+  const R usqc = nadd(nadd(nmul(uxc, uxc), nmul(uyc, uyc)), nmul(uzn, uzn));
+  static_for<18>([&](auto Qm1) {
+    constexpr int q = Qm1 + 1;
+    constexpr int cx = kC19[q][0], cy = kC19[q][1], cz = kC19[q][2];
+    if constexpr (cx != 0 || cy != 0) {
+      if (!(cz == -1 && top) && lateral_out<cx, cy>(C)) {
+        const R w = R(w19(q));
+        if (inflow_cond<cx, cy>(C, P)) {
+          const R cu = cdot<R, cx, cy, 0>(uI, vI, R(0));
+          f[q] = nmul(w, feq_poly(cu, nadd(nmul(uI, uI), nmul(vI, vI))));
+        } else {
+          const R cu = cdot<R, cx, cy, cz>(uxn, uyn, uzn);
+          if (P.oclip != 0) {
+            const R cuc = cdot<R, cx, cy, cz>(uxc, uyc, uzn);
+            f[q] = nadd(f[q], nmul(w, nsub(feq_poly(cuc, usqc), nmul(rn, feq_poly(cu, usqn)))));
+          } else {
+            f[q] = nadd(f[q], nmul(nmul(w, nsub(R(1.0), rn)), feq_poly(cu, usqn)));
+          }
+        }
+      }
+    }
+  });
+  static_for<6>([&](auto Qm1) {
+    constexpr int q = Qm1 + 1;
+    constexpr int cx = kC7[q][0], cy = kC7[q][1], cz = kC7[q][2];
+    if constexpr (cx != 0 || cy != 0) {
+      if (!(cz == -1 && top) && lateral_out<cx, cy>(C) && inflow_cond<cx, cy>(C, P)) g[q] = R(0);
+    }
+  });
+}
+
 // secProfile + secOutflowPrelude + secStreamF + secStreamG for cell (C.i, C.j, k); n is the pitched cell index.
 template <class S>
 __device__ __forceinline__ void stream_cell(const DomainView& D, const ParamsHead& P, const float4* prof,
@@ -239,61 +306,7 @@ __device__ __forceinline__ void stream_cell(const DomainView& D, const ParamsHea
     X.g[q] = KG::dec_g(KG::load(gA + off));
   });
 
-  if (C.face) {
-    // secOutflowPrelude (kernel.js:122-148): own-cell density and velocity on outflow faces
-    R rn = R(1), uxn = R(0), uyn = R(0), uzn = R(0);
-    if (C.onb) {
-      R own[19];
-      static_for<19>([&](auto Q) {
-        constexpr int q = Q;
-        own[q] = KF::dec_f(KF::load(fA + (uint32_t)q * qs + n), R(w19(q)));
-      });
-      rn = own[0];
-#pragma unroll
-      for (int q = 1; q < 19; ++q) rn = rn + own[q];
-      auto fo = [&](int q) { return own[q]; };
-      uxn = moment1<R, 0>(fo) / rn;
-      uyn = moment1<R, 1>(fo) / rn;
-      uzn = moment1<R, 2>(fo) / rn;
-    }
-    const R usqn = nadd(nadd(nmul(uxn, uxn), nmul(uyn, uyn)), nmul(uzn, uzn));
-    R uxc = uxn, uyc = uyn;
-    if (P.oclip != 0) {
-      if (C.latW && P.inflow_w == 0 && uxc > R(0)) uxc = R(0);
-      if (C.latE && P.inflow_e == 0 && uxc < R(0)) uxc = R(0);
-      if (C.latS && P.inflow_s == 0 && uyc > R(0)) uyc = R(0);
-      if (C.latN && P.inflow_n == 0 && uyc < R(0)) uyc = R(0);
-    }
-    const R usqc = nadd(nadd(nmul(uxc, uxc), nmul(uyc, uyc)), nmul(uzn, uzn));
-    static_for<18>([&](auto Qm1) {
-      constexpr int q = Qm1 + 1;
-      constexpr int cx = kC19[q][0], cy = kC19[q][1], cz = kC19[q][2];
-      if constexpr (cx != 0 || cy != 0) {
-        if (!(cz == -1 && top) && lateral_out<cx, cy>(C)) {
-          const R w = R(w19(q));
-          if (inflow_cond<cx, cy>(C, P)) {
-            const R cu = cdot<R, cx, cy, 0>(uI, vI, R(0));
-            X.f[q] = nmul(w, feq_poly(cu, nadd(nmul(uI, uI), nmul(vI, vI))));
-          } else {
-            const R cu = cdot<R, cx, cy, cz>(uxn, uyn, uzn);
-            if (P.oclip != 0) {
-              const R cuc = cdot<R, cx, cy, cz>(uxc, uyc, uzn);
-              X.f[q] = nadd(X.f[q], nmul(w, nsub(feq_poly(cuc, usqc), nmul(rn, feq_poly(cu, usqn)))));
-            } else {
-              X.f[q] = nadd(X.f[q], nmul(nmul(w, nsub(R(1.0), rn)), feq_poly(cu, usqn)));
-            }
-          }
-        }
-      }
-    });
-    static_for<6>([&](auto Qm1) {
-      constexpr int q = Qm1 + 1;
-      constexpr int cx = kC7[q][0], cy = kC7[q][1], cz = kC7[q][2];
-      if constexpr (cx != 0 || cy != 0) {
-        if (!(cz == -1 && top) && lateral_out<cx, cy>(C) && inflow_cond<cx, cy>(C, P)) X.g[q] = R(0);
-      }
-    });
-  }
+  if (C.face) face_patch<S>(D, P, C, top, n, uI, vI, X.f, X.g);
 }
 
 // Interior cells (not on a lateral face, below the lid, every source fluid): the stream is a plain gather, one load
@@ -583,8 +596,6 @@ template <class S>
 __device__ __forceinline__ void fast_pair(const DomainView& D, const ParamsHead& P, const RelaxConst& RK,
                                           const float4* prof, const Column<float>& C, int k, uint32_t n, uint32_t r0,
                                           uint32_t r1) {
-  const StoreF<S>* fA = static_cast<const StoreF<S>*>(D.fA);
-  const StoreG<S>* gA = static_cast<const StoreG<S>*>(D.gA);
   StoreF<S>* fB = static_cast<StoreF<S>*>(D.fB);
   StoreG<S>* gB = static_cast<StoreG<S>*>(D.gB);
   const uint32_t ps = D.ps;
@@ -681,8 +692,13 @@ __device__ __forceinline__ void step_block(const DomainView& D, int bx, int by, 
   const ParamsHead& P = sP;
   const RelaxConst RK = relax_const(P);
 
-  const int i = bx * kBlockX + threadIdx.x;
-  const int j = D.jbase + by * (int)blockDim.y + (int)threadIdx.y;
+  // role of the block (step_split): the main blocks cover their rows' main columns as warps of 32 consecutive
+  // columns; the strip blocks after them give each thread one strip column
+  const StepSplit SP = step_split(D.nx, D.jlo, D.jhi, D.jbase, D.jg0, D.nyg, D.strip);
+  const bool strip_block = by >= main_blocks_y(D.jhi, D.jbase, (int)blockDim.y);
+  int i, j;
+  const bool valid = block_column(SP, D.nx, D.jbase, D.jhi, (int)blockDim.y, bx, by, (int)threadIdx.x,
+                                  (int)threadIdx.y, i, j);
   const int k0 = bz * zslab;
   const int k1 = min(D.nz, k0 + zslab);
   BudgetAcc B;
@@ -694,7 +710,6 @@ __device__ __forceinline__ void step_block(const DomainView& D, int bx, int by, 
   // A warp is one row of 32 columns. It walks the levels in lockstep from its lowest first fluid level, so the lanes
   // of one load touch one level (coalesced), and it takes the interior fast path only when every active lane is
   // interior (the general path gives identical values for interior cells, so a mixed level runs one path, not two).
-  const bool valid = i < D.nx && j >= D.jlo && j < D.jhi;
   Column<R> C;
   int kstart = k1;
   if (valid) {
@@ -719,12 +734,12 @@ __device__ __forceinline__ void step_block(const DomainView& D, int bx, int by, 
   constexpr bool kPairs = PAIRS && FAST && MODE == 0 && !BUDGET && std::is_same_v<R, float>;
   // FMA build, plain steps, launch option: the next level's (pair's) source rows are prefetched into L2 one level
   // (pair) ahead
-  constexpr bool kPrefetch = FAST && MODE == 0 && !BUDGET;
-  const uint32_t rowbase = (uint32_t)j * (uint32_t)D.px + (uint32_t)(bx * kBlockX);
+  constexpr bool kPrefetch = FAST && MODE == 0 && !BUDGET;   // (main blocks only: strip lanes are not one row)
+  const uint32_t rowbase = (uint32_t)j * (uint32_t)D.px + (uint32_t)(SP.we + bx * kBlockX);
 #pragma unroll 1
   for (int k = kw; k < k1; ++k) {
     if constexpr (kPrefetch) {
-      if (D.pf) {
+      if (D.pf && !strip_block) {
         if (k + (kPairs ? 2 : 1) < k1) prefetch_level<S>(D, k + (kPairs ? 2 : 1), rowbase);
         if (kPairs && k + 3 < k1) prefetch_level<S>(D, k + 3, rowbase);
       }

@@ -9,6 +9,8 @@
 #include <cuda_fp16.h>
 #include <stdint.h>
 
+#include "split.h"
+
 #include <type_traits>
 #include <utility>
 
@@ -303,6 +305,7 @@ struct DomainView {
   // others are ghost rows refreshed from the neighbouring slabs); a whole domain has jg0 0, nyg ny, [0, ny)
   int jg0, nyg, jlo, jhi;
   int jbase;                    // first local row the launch's grid covers (0 unless a step of a band of rows)
+  int strip;                    // strip width of the column split (step_split)
   uint32_t ps;                  // plane stride px*ny
   uint32_t qs;                  // q stride px*ny*nz
   // element offset of the interior pull source of population q relative to the cell: q*qs - (cx + cy*px + cz*ps)

@@ -163,8 +163,10 @@ static cudaError_t launch_t(const DomainView& D, const StepLaunch& L, cudaStream
   const int by = minb ? 4 : (L.block_y > 0 ? L.block_y : 4);
   const int zs = L.zslab > 0 ? L.zslab : D.nz;
   dim3 block(kBlockX, by);
-  // the rows [jbase, jhi) the step updates (all rows, unless a slab or a band of rows)
-  dim3 grid((D.nx + kBlockX - 1) / kBlockX, (D.jhi - D.jbase + by - 1) / by, (D.nz + zs - 1) / zs);
+  // the rows [jbase, jhi) the step updates (all rows, unless a slab or a band of rows): the main blocks, then the
+  // strip blocks (step_split)
+  const StepSplit SP = step_split(D.nx, D.jlo, D.jhi, D.jbase, D.jg0, D.nyg, D.strip);
+  dim3 grid(SP.gx, main_blocks_y(D.jhi, D.jbase, by) + strip_blocks_y(SP, by), (D.nz + zs - 1) / zs);
   const size_t smem = (size_t)D.nz * sizeof(float4);
   if constexpr (MODE == 0 && !BUDGET && AHX_STEP_FAST != 0 && std::is_same_v<RealOf<S>, float>) {
     if (L.pairs) {
