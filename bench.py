@@ -234,6 +234,64 @@ def run_reference(a, rank):
     return 0
 
 
+def secondary_rates(a, local):
+    """Further device-timed measurements of the same run on one GPU, after the headline: the 16-bit storages on the
+    same domain (FMA build, each on its own tuned launch; algorithmic bytes 104 B per fluid cell), and the 64-domain
+    batched ensemble of the c4 workload (one batched launch sequence per step, against the same members stepped one
+    after another)."""
+    from ashburn_heat_twin_b200 import LiveBatch
+    from ashburn_heat_twin_b200 import scenarios as SC
+    from ashburn_heat_twin_b200 import solver as S
+    from ashburn_heat_twin_b200 import synth
+    from ashburn_heat_twin_b200.cuda_device import CudaDevice
+    peak, peak_kind = measured_peaks()
+    out = {}
+    for p in ('fp16', 'fp16sr'):
+        s = make_solver(device=local, precision=p, arith='fast', workload=a.workload)
+        by, zs, _ = s._dev.autotune(3)
+        s._dev.time_steps(a.warmup)
+        ms = s._dev.time_steps(a.steps) / a.steps
+        cells, fluid = s.info['nCells'], s.info['nFluid']
+        out[p] = dict(glups=cells / ms / 1e6, ms_per_step=ms, launch=dict(block_y=by, zslab=zs),
+                      roofline=dict(bound='hbm', achieved=fluid * CELL_BYTES[p] / (ms / 1e3) / 1e9, peak=peak,
+                                    unit='GB/s', frac=fluid * CELL_BYTES[p] / (ms / 1e3) / 1e9 / peak,
+                                    peak_source=peak_kind),
+                      dtype=DTYPE[p])
+        s.destroy()
+    st = synth.make_static10(synth.C1)
+    scen = SC.batch64(st)
+
+    def backend(nx, ny, nz):
+        return CudaDevice(nx, ny, nz, device=local, precision='fp32', arith='fast')
+    solvers = []
+    for c in scen:
+        s = S.create_live_solver(backend=backend, static=st, dx=c['dx'], heightM=c['heightM'], u10Max=8, met=c['met'],
+                                 existingFlux=c['flux'])
+        s.setNewCampuses([c['campus']])
+        solvers.append(s)
+    classes = {}
+    for s in solvers:
+        classes.setdefault((s.info['nx'], s.info['ny'], s.info['nz']), []).append(s)
+    for members in classes.values():
+        by, zs, _ = members[0]._dev.autotune(3)
+        for m in members[1:]:
+            m._dev.set_launch(by, zs)
+    b = LiveBatch(solvers)
+    btune = b.autotune(4)
+    b._b.time_steps(a.warmup)
+    ms = b._b.time_steps(a.steps) / a.steps
+    serial_ms = sum(s._dev.time_steps(a.steps) for s in solvers) / a.steps
+    cells = sum(s.info['nCells'] for s in solvers)
+    fluid = sum(s.info['nFluid'] for s in solvers)
+    b.destroy()
+    for s in solvers:
+        s.destroy()
+    out['batch64'] = dict(workload=WORKLOADS['c4']['desc'], glups=cells / ms / 1e6, ms_per_step=ms,
+                          serial_glups=cells / serial_ms / 1e6, over_serial=serial_ms / ms, tuned=btune,
+                          roofline_frac=fluid * 208 / (ms / 1e3) / 1e9 / peak, dtype='f32')
+    return out
+
+
 def main_batch(a, rank, world, local, dist, torch):
     """The batched workload: 64 seeded domains stepped by one persistent launch per step (a CUDA graph replays two
     steps); launch shapes tuned per grid class on scratch copies, then the batch's own variant and tile depth.
@@ -650,6 +708,8 @@ def main():
     ap.add_argument('--frame', type=int, default=10, help='steps per e2e frame (setMet + step(F) + read())')
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--no-autotune', action='store_true')
+    ap.add_argument('--no-secondary', action='store_true',
+                    help='skip the further rates of the default run (16-bit storages, 64-domain batch)')
     ap.add_argument('--block-y', type=int, default=0, help='fix the launch shape instead of autotuning')
     ap.add_argument('--zslab', type=int, default=0)
     ap.add_argument('--workload', default='c2', choices=sorted(WORKLOADS),
@@ -788,6 +848,14 @@ def main():
         s_steps = s._steps
         cpu = cpu_baseline(workload=a.workload)
         del s_steps
+    state_bytes = s._dev.info()['state_bytes']
+    more = None
+    if world == 1 and not a.no_secondary and a.workload == 'c2' and a.precision == 'fp32':
+        s.destroy()
+        s = None
+        with Clocks(local) as clk2:
+            more = secondary_rates(a, local)
+        more['clocks'] = clk2.summary()
     metric = METRIC.replace('600x600x64', f'{nx}x{ny}x{nz}')
     vs = value / wl['published_glups'] if wl.get('published_glups') else None
     out = dict(metric=metric, value=value, unit='GLUPS', n_gpus=world, steps=a.steps, warmup=a.warmup,
@@ -796,12 +864,13 @@ def main():
                data=('the reference\'s own Ashburn planes (tests/golden/static10.*)' if wl.get('real') else
                      'synthetic (seeded terrain and buildings; no public dataset involved)'),
                config=bench_config(a.workload, a.precision, cells),
-               arith=a.arith, fluid_cells=fluid, replicas=world, state_bytes=s._dev.info()['state_bytes'],
+               arith=a.arith, fluid_cells=fluid, replicas=world, state_bytes=state_bytes,
                launch=dict(block_y=launch_used[0], zslab=launch_used[1], tuned=tune is not None and tune[2] is not None),
                published=wl.get('published'),
                roofline=roof, cpu_baseline=cpu, e2e=e2e, read_ms=read_ms, gpu_launches=a.steps, clocks=clocks,
-               glups_fluid=world * fluid * a.steps / (ms_all / 1e3) / 1e9)
-    s.destroy()
+               glups_fluid=world * fluid * a.steps / (ms_all / 1e3) / 1e9, secondary=more)
+    if s is not None:
+        s.destroy()
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
