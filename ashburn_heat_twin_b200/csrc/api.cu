@@ -91,7 +91,7 @@ DomainView ahx::view_at(ahx_handle* h, int parity) {
   D.strip = strip_width(h->esize);
   D.ps = h->ps;
   D.qs = h->qs;
-  set_offsets(D);
+  set_offsets(D, h->esize, h->esize_g);
   set_pointers(D, h->esize, h->esize_g);
   return D;
 }
@@ -306,7 +306,9 @@ ahx_status ahx_create(const ahx_dims* dims, ahx_handle** out) {
   const int align = 128 / esize;   // x rows start on 128-byte boundaries
   const int px = (dims->nx + align - 1) / align * align;
   const uint64_t ps = (uint64_t)px * dims->ny;
-  const uint64_t qs = ps * dims->nz;
+  // a level-paired (16-bit) population plane holds nz rounded up to even levels (lvl)
+  const bool paired = esize == 2 || element_bytes_g(dims->precision) == 2;
+  const uint64_t qs = ps * (uint64_t)(paired ? dims->nz + (dims->nz & 1) : dims->nz);
   if (19 * qs >= (1ull << 32))
     return fail(AHX_EINVAL, "live solver: grid too large for one handle (19 population planes must index in 32 bits)");
   int ndev = 0;
@@ -360,7 +362,8 @@ ahx_status ahx_create(const ahx_dims* dims, ahx_handle** out) {
   cudaMemsetAsync(h->d_err, 0, sizeof(int), h->s_step);
   cudaMemsetAsync(h->d_tick, 0, 4 * sizeof(uint32_t), h->s_step);
   // the staged kernel stages f and g with one element size and rounds to nearest
-  h->maps_ok = h->esize == h->esize_g && dims->precision != AHX_FP16_SR;
+  // staged boxes are single levels of 4- and 8-byte planes
+  h->maps_ok = h->esize == h->esize_g && h->esize != 2 && dims->precision != AHX_FP16_SR;
   for (int t = 0; t < 2 && h->maps_ok; ++t)
     for (int p = 0; p < 2; ++p) h->maps_ok = h->maps_ok && make_maps(h, h->f[p], h->g[p], t ? 8 : 4, &h->maps[t][p]);
   cudaMemsetAsync(h->d_params, 0, 64 + 16 * (size_t)dims->nz, h->s_step);

@@ -55,9 +55,8 @@ __global__ void __launch_bounds__(128) surf_kernel(DomainView D, float conv, flo
   }
   Column<R> C;
   load_column(D, sP, i, j, C);
-  const uint32_t n = (uint32_t)k * D.ps + (uint32_t)j * (uint32_t)D.px + (uint32_t)i;
   Cell<R> X;
-  stream_cell<S>(D, sP, prof, C, k, n, X);
+  stream_cell<S>(D, sP, prof, C, k, (uint32_t)j * (uint32_t)D.px + (uint32_t)i, X);
   Macro<R> M;
   moments_forces<R>(sP, C, k, D.nz, X, M);
   sout[o] = (float)M.th;
@@ -100,7 +99,8 @@ __global__ void __launch_bounds__(256) vol_kernel(DomainView D, int nzv, float v
         const int kg = (int)__ldg(D.ktop + (long)j * nx + i);
         R th = R(0);
         if (k >= kg) {
-          const uint32_t n = (uint32_t)k * D.ps + (uint32_t)j * (uint32_t)D.px + (uint32_t)i;
+          using TG = StoreG<S>;
+          const uint32_t m = (uint32_t)j * (uint32_t)D.px + (uint32_t)i, n = lvl<TG>(k, m, D.ps);
           R g[7];
           g[0] = KG::dec_g(KG::load(gA + n));
           static_for<6>([&](auto Qm1) {
@@ -121,7 +121,7 @@ __global__ void __launch_bounds__(256) vol_kernel(DomainView D, int nzv, float v
               gv = KG::dec_g(KG::load(gA + (uint32_t)opp7(q) * D.qs + n));
             } else {
               // the offset wraps in 32 bits before it touches the pointer (cx = -1 gives a negative shift)
-              const uint32_t off = (uint32_t)q * D.qs + n - (uint32_t)(cx + cy * D.px + cz * (int)D.ps);
+              const uint32_t off = (uint32_t)q * D.qs + lvl<TG>(sk, m - (uint32_t)(cx + cy * D.px), D.ps);
               gv = KG::dec_g(KG::load(gA + off));
             }
             g[q] = gv;
@@ -165,7 +165,7 @@ __global__ void __launch_bounds__(256) init_kernel(DomainView D, StoreF<S>* f0, 
   const float4 pr = __ldg(prof + zagl);
   const R U = R(pr.x), V = R(pr.y);
   const R usq = U * U + V * V;
-  const uint32_t n = (uint32_t)k * D.ps + (uint32_t)j * (uint32_t)D.px + (uint32_t)i;
+  const uint32_t n = lvl<StoreF<S>>(k, (uint32_t)j * (uint32_t)D.px + (uint32_t)i, D.ps);
   static_for<19>([&](auto Q) {
     constexpr int q = Q;
     const R cu = R(kC19[q][0]) * U + R(kC19[q][1]) * V;
@@ -190,14 +190,15 @@ __global__ void __launch_bounds__(256) reinit_kernel(DomainView D, const uint32_
   const int i = c % D.nx, j = c / D.nx;
   const int k1 = min((int)oldk[c], D.nz);
   for (int k = (int)D.ktop[c]; k < k1; ++k) {
-    const uint32_t n = (uint32_t)k * D.ps + (uint32_t)j * (uint32_t)D.px + (uint32_t)i;
+    const uint32_t m = (uint32_t)j * (uint32_t)D.px + (uint32_t)i;
+    const uint32_t nf = lvl<StoreF<S>>(k, m, D.ps), ng = lvl<StoreG<S>>(k, m, D.ps);
     static_for<19>([&](auto Q) {
       constexpr int q = Q;
-      f[(uint32_t)q * D.qs + n] = KF::enc_f(R(w19(q)), R(w19(q)));
+      f[(uint32_t)q * D.qs + nf] = KF::enc_f(R(w19(q)), R(w19(q)));
     });
     static_for<7>([&](auto Q) {
       constexpr int q = Q;
-      g[(uint32_t)q * D.qs + n] = KG::enc_g(R(0));
+      g[(uint32_t)q * D.qs + ng] = KG::enc_g(R(0));
     });
   }
 }
@@ -222,20 +223,21 @@ __global__ void __launch_bounds__(256) stats_kernel(DomainView D, StatsScratch* 
     const int k = (int)(c / ((long)nx * ny));
     if (j < D.jlo || j >= D.jhi) continue;   // ghost rows of a slab belong to its neighbour
     if (k < (int)__ldg(D.ktop + (long)j * nx + i)) continue;
-    const uint32_t n = (uint32_t)k * D.ps + (uint32_t)j * (uint32_t)D.px + (uint32_t)i;
+    const uint32_t m = (uint32_t)j * (uint32_t)D.px + (uint32_t)i;
+    const uint32_t nf = lvl<StoreF<S>>(k, m, D.ps), ng = lvl<StoreG<S>>(k, m, D.ps);
     R f[19];
     static_for<19>([&](auto Q) {
       constexpr int q = Q;
-      f[q] = KF::dec_f(KF::load(fA + (uint32_t)q * D.qs + n), R(w19(q)));
+      f[q] = KF::dec_f(KF::load(fA + (uint32_t)q * D.qs + nf), R(w19(q)));
     });
     float rho = (float)f[0];
 #pragma unroll
     for (int q = 1; q < 19; ++q) rho = rho + (float)f[q];
     auto fq = [&](int q) { return (float)f[q]; };
     const float jx = moment1<float, 0>(fq), jy = moment1<float, 1>(fq), jz = moment1<float, 2>(fq);
-    float th = (float)KG::dec_g(KG::load(gA + n));
+    float th = (float)KG::dec_g(KG::load(gA + ng));
 #pragma unroll
-    for (int q = 1; q < 7; ++q) th = th + (float)KG::dec_g(KG::load(gA + (uint32_t)q * D.qs + n));
+    for (int q = 1; q < 7; ++q) th = th + (float)KG::dec_g(KG::load(gA + (uint32_t)q * D.qs + ng));
     const unsigned br = __float_as_uint(rho) & 0x7f800000u, bt = __float_as_uint(th) & 0x7f800000u;
     if (br == 0x7f800000u || bt == 0x7f800000u) {
       ++nonf;
@@ -283,7 +285,7 @@ __global__ void __launch_bounds__(256) import_plane_kernel(DomainView D, const v
   const size_t c = ((size_t)k * D.ny + j) * D.nx + i;
   const R v = ref_is_f64 ? R(static_cast<const double*>(ref)[c]) : R(static_cast<const float*>(ref)[c]);
   const double w = q == 0 ? 1.0 / 3 : (q < 7 ? 1.0 / 18 : 1.0 / 36);
-  const uint32_t n = (uint32_t)k * D.ps + (uint32_t)j * (uint32_t)D.px + (uint32_t)i;
+  const uint32_t n = lvl<T>(k, (uint32_t)j * (uint32_t)D.px + (uint32_t)i, D.ps);
   dst[(uint32_t)q * D.qs + n] = is_g ? K::enc_g(v) : K::enc_f(v, R(w));
 }
 
@@ -297,7 +299,7 @@ __global__ void __launch_bounds__(256) export_plane_kernel(DomainView D, const T
   if (i >= D.nx) return;
   const size_t c = ((size_t)k * D.ny + j) * D.nx + i;
   const double w = q == 0 ? 1.0 / 3 : (q < 7 ? 1.0 / 18 : 1.0 / 36);
-  const uint32_t n = (uint32_t)k * D.ps + (uint32_t)j * (uint32_t)D.px + (uint32_t)i;
+  const uint32_t n = lvl<T>(k, (uint32_t)j * (uint32_t)D.px + (uint32_t)i, D.ps);
   const T e = src[(uint32_t)q * D.qs + n];
   const R v = is_g ? K::dec_g(e) : K::dec_f(e, R(w));
   if (ref_is_f64) static_cast<double*>(ref)[c] = (double)v;
@@ -314,14 +316,14 @@ __global__ void __launch_bounds__(256) row_copy_kernel(DomainView D, int j, cons
   if (e >= 26 * per) return;
   const int q = (int)(e / per);
   const int k = (int)((e % per) / D.nx), i = (int)(e % D.nx);
-  const uint32_t n = (uint32_t)k * D.ps + (uint32_t)j * (uint32_t)D.px + (uint32_t)i;
+  const uint32_t m = (uint32_t)j * (uint32_t)D.px + (uint32_t)i;
   if (q < 19) {
-    TF* s = const_cast<TF*>(static_cast<const TF*>(f)) + (uint32_t)q * D.qs + n;
+    TF* s = const_cast<TF*>(static_cast<const TF*>(f)) + (uint32_t)q * D.qs + lvl<TF>(k, m, D.ps);
     TF* b = static_cast<TF*>(buf) + (long)q * per + (long)k * D.nx + i;
     if (to_buffer) *b = *s;
     else *s = *b;
   } else {
-    TG* s = const_cast<TG*>(static_cast<const TG*>(g)) + (uint32_t)(q - 19) * D.qs + n;
+    TG* s = const_cast<TG*>(static_cast<const TG*>(g)) + (uint32_t)(q - 19) * D.qs + lvl<TG>(k, m, D.ps);
     // the g part starts at the next 16-byte boundary after the f part
     const size_t goff = (19 * (size_t)per * sizeof(TF) + 15) & ~(size_t)15;
     TG* b = reinterpret_cast<TG*>(static_cast<unsigned char*>(buf) + goff) + (long)(q - 19) * per + (long)k * D.nx + i;
@@ -356,15 +358,15 @@ __global__ void __launch_bounds__(256) halo_copy_kernel(DomainView D, int j, con
   if (e >= 6 * per) return;
   const int slot = (int)(e / per);
   const int k = (int)((e % per) / D.nx), i = (int)(e % D.nx);
-  const uint32_t n = (uint32_t)k * D.ps + (uint32_t)j * (uint32_t)D.px + (uint32_t)i;
+  const uint32_t m = (uint32_t)j * (uint32_t)D.px + (uint32_t)i;
   constexpr HaloPlanes H = halo_planes(DIR);
   if (slot < 5) {
-    TF* s = const_cast<TF*>(static_cast<const TF*>(f)) + (uint32_t)H.f[slot] * D.qs + n;
+    TF* s = const_cast<TF*>(static_cast<const TF*>(f)) + (uint32_t)H.f[slot] * D.qs + lvl<TF>(k, m, D.ps);
     TF* b = static_cast<TF*>(buf) + (long)slot * per + (long)k * D.nx + i;
     if (to_buffer) *b = *s;
     else *s = *b;
   } else {
-    TG* s = const_cast<TG*>(static_cast<const TG*>(g)) + (uint32_t)H.g * D.qs + n;
+    TG* s = const_cast<TG*>(static_cast<const TG*>(g)) + (uint32_t)H.g * D.qs + lvl<TG>(k, m, D.ps);
     const size_t goff = (5 * (size_t)per * sizeof(TF) + 15) & ~(size_t)15;
     TG* b = reinterpret_cast<TG*>(static_cast<unsigned char*>(buf) + goff) + (long)k * D.nx + i;
     if (to_buffer) *b = *s;

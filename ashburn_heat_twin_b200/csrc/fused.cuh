@@ -180,10 +180,11 @@ __device__ __forceinline__ R feq_poly(R cu, R usq) {
 // The lateral-face rules of the stream for a cell of a face column (C.face), after its populations were loaded with
 // every outside source taken from the own cell: secOutflowPrelude (kernel.js:122-148) and the in/outflow cases of
 // secStreamF / secStreamG (kernel.js:187-204, 219-243). f and g are the decoded populations of cell n at level k (top:
-// k is the lid level). The formulas use non-contractible operations, so every kernel path gives the same bits.
+// k is the lid level); nf is the cell's own element offset in an f plane (lvl). The formulas use non-contractible
+// operations, so every kernel path gives the same bits.
 template <class S>
 __device__ __forceinline__ void face_patch(const DomainView& D, const ParamsHead& P, const Column<RealOf<S>>& C,
-                                           bool top, uint32_t n, RealOf<S> uI, RealOf<S> vI, RealOf<S> (&f)[19],
+                                           bool top, uint32_t nf, RealOf<S> uI, RealOf<S> vI, RealOf<S> (&f)[19],
                                            RealOf<S> (&g)[7]) {
   using R = RealOf<S>;
   using KF = CodecF<S>;
@@ -195,7 +196,7 @@ __device__ __forceinline__ void face_patch(const DomainView& D, const ParamsHead
     R own[19];
     static_for<19>([&](auto Q) {
       constexpr int q = Q;
-      own[q] = KF::dec_f(KF::load(fA + (uint32_t)q * qs + n), R(w19(q)));
+      own[q] = KF::dec_f(KF::load(fA + (uint32_t)q * qs + nf), R(w19(q)));
     });
     rn = own[0];
 #pragma unroll
@@ -244,17 +245,21 @@ __device__ __forceinline__ void face_patch(const DomainView& D, const ParamsHead
   });
 }
 
-// secProfile + secOutflowPrelude + secStreamF + secStreamG for cell (C.i, C.j, k); n is the pitched cell index.
+// secProfile + secOutflowPrelude + secStreamF + secStreamG for cell (C.i, C.j, k); m = j px + i is the cell's
+// row-column index in a level (element offsets through lvl).
 template <class S>
 __device__ __forceinline__ void stream_cell(const DomainView& D, const ParamsHead& P, const float4* prof,
-                                            const Column<RealOf<S>>& C, int k, uint32_t n,
+                                            const Column<RealOf<S>>& C, int k, uint32_t m,
                                             Cell<RealOf<S>>& X) {
   using R = RealOf<S>;
   using KF = CodecF<S>;
   using KG = CodecG<S>;
   const StoreF<S>* fA = static_cast<const StoreF<S>*>(D.fA);
   const StoreG<S>* gA = static_cast<const StoreG<S>*>(D.gA);
+  using TF = StoreF<S>;
+  using TG = StoreG<S>;
   const uint32_t qs = D.qs, ps = D.ps, px = (uint32_t)D.px;
+  const uint32_t nf = lvl<TF>(k, m, ps), ng = lvl<TG>(k, m, ps);
   const bool top = (k == D.nz - 1);
   // secProfile
   int zagl = k - C.ktc;
@@ -267,7 +272,7 @@ __device__ __forceinline__ void stream_cell(const DomainView& D, const ParamsHea
   X.kb = R(pr.z);
 
   // secStreamF / secStreamG as an index remap: one load per population
-  X.f[0] = KF::dec_f(KF::load(fA + n), R(w19(0)));
+  X.f[0] = KF::dec_f(KF::load(fA + nf), R(w19(0)));
   static_for<18>([&](auto Qm1) {
     constexpr int q = Qm1 + 1;
     constexpr int cx = kC19[q][0], cy = kC19[q][1], cz = kC19[q][2];
@@ -277,19 +282,19 @@ __device__ __forceinline__ void stream_cell(const DomainView& D, const ParamsHea
     if (cz == -1 && top) {
       // free-slip lid: the z-mirrored population from the same layer, or the own cell's when the lateral source
       // is outside or solid (kernel.js:168-181)
-      constexpr int m = mirz19(q);
+      constexpr int mz = mirz19(q);
       const bool own = lat || (k < C.kn[1 - cx][1 - cy]);
-      off = (uint32_t)m * qs + (own ? n : n - (uint32_t)(cx + cy * (int)px));
+      off = (uint32_t)mz * qs + (own ? nf : lvl_nbr<TF>(k, m, nf, 0, (uint32_t)(cx + cy * (int)px), ps));
     } else if (lat) {
-      off = (uint32_t)q * qs + n;   // in/outflow: patched below from the own value
+      off = (uint32_t)q * qs + nf;   // in/outflow: patched below from the own value
     } else if (sk < C.kn[1 - cx][1 - cy]) {
-      off = (uint32_t)opp19(q) * qs + n;   // half-way bounce-back (kernel.js:209-210)
+      off = (uint32_t)opp19(q) * qs + nf;   // half-way bounce-back (kernel.js:209-210)
     } else {
-      off = (uint32_t)q * qs + n - (uint32_t)(cx + cy * (int)px + cz * (int)ps);
+      off = (uint32_t)q * qs + lvl_nbr<TF>(k, m, nf, cz, (uint32_t)(cx + cy * (int)px), ps);
     }
     X.f[q] = KF::dec_f(KF::load(fA + off), R(w19(q)));
   });
-  X.g[0] = KG::dec_g(KG::load(gA + n));
+  X.g[0] = KG::dec_g(KG::load(gA + ng));
   static_for<6>([&](auto Qm1) {
     constexpr int q = Qm1 + 1;
     constexpr int cx = kC7[q][0], cy = kC7[q][1], cz = kC7[q][2];
@@ -297,29 +302,30 @@ __device__ __forceinline__ void stream_cell(const DomainView& D, const ParamsHea
     const bool lat = lateral_out<cx, cy>(C);
     uint32_t off;
     if ((cz == -1 && top) || lat) {
-      off = (uint32_t)q * qs + n;   // zero-gradient lid / outflow: own value; inflow patched to 0 below
+      off = (uint32_t)q * qs + ng;   // zero-gradient lid / outflow: own value; inflow patched to 0 below
     } else if (sk < C.kn[1 - cx][1 - cy]) {
-      off = (uint32_t)opp7(q) * qs + n;
+      off = (uint32_t)opp7(q) * qs + ng;
     } else {
-      off = (uint32_t)q * qs + n - (uint32_t)(cx + cy * (int)px + cz * (int)ps);
+      off = (uint32_t)q * qs + lvl_nbr<TG>(k, m, ng, cz, (uint32_t)(cx + cy * (int)px), ps);
     }
     X.g[q] = KG::dec_g(KG::load(gA + off));
   });
 
-  if (C.face) face_patch<S>(D, P, C, top, n, uI, vI, X.f, X.g);
+  if (C.face) face_patch<S>(D, P, C, top, nf, uI, vI, X.f, X.g);
 }
 
 // Interior cells (not on a lateral face, below the lid, every source fluid): the stream is a plain gather, one load
-// per population at a fixed offset; loads exactly the values stream_cell would.
+// per population at a fixed offset (level-paired planes: the source's lvl offset, which depends on the parity of the
+// level); loads exactly the values stream_cell would.
 template <class S>
 __device__ __forceinline__ void stream_interior(const DomainView& D, const float4* prof,
-                                                const Column<RealOf<S>>& C, int k, uint32_t n,
+                                                const Column<RealOf<S>>& C, int k, uint32_t m,
                                                 Cell<RealOf<S>>& X) {
   using R = RealOf<S>;
   using KF = CodecF<S>;
   using KG = CodecG<S>;
-  const StoreF<S>* fA = static_cast<const StoreF<S>*>(D.fA);
-  const StoreG<S>* gA = static_cast<const StoreG<S>*>(D.gA);
+  using TF = StoreF<S>;
+  using TG = StoreG<S>;
   int zagl = k - C.ktc;
   if (zagl < 0) zagl = 0;
   if (zagl > D.nz - 1) zagl = D.nz - 1;
@@ -327,13 +333,25 @@ __device__ __forceinline__ void stream_interior(const DomainView& D, const float
   X.uI = R(pr.x);
   X.vI = R(pr.y);
   X.kb = R(pr.z);
+  const uint32_t ps = D.ps, px = (uint32_t)D.px, n = (uint32_t)k * ps + m;
   static_for<19>([&](auto Q) {
     constexpr int q = Q;
-    X.f[q] = KF::dec_f(KF::load(static_cast<const StoreF<S>*>(D.src_f[q]) + n), R(w19(q)));
+    [[maybe_unused]] constexpr int cx = kC19[q][0], cy = kC19[q][1], cz = kC19[q][2];
+    if constexpr (kLevelPairs<TF>)
+      X.f[q] = KF::dec_f(KF::load(static_cast<const TF*>(D.fA) +
+                                  ((uint32_t)q * D.qs + lvl_nbr<TF>(k, m, 0u, cz, (uint32_t)(cx + cy * (int)px), ps))),
+                         R(w19(q)));
+    else
+      X.f[q] = KF::dec_f(KF::load(static_cast<const TF*>(D.src_f[q]) + n), R(w19(q)));
   });
   static_for<7>([&](auto Q) {
     constexpr int q = Q;
-    X.g[q] = KG::dec_g(KG::load(static_cast<const StoreG<S>*>(D.src_g[q]) + n));
+    [[maybe_unused]] constexpr int cx = kC7[q][0], cy = kC7[q][1], cz = kC7[q][2];
+    if constexpr (kLevelPairs<TG>)
+      X.g[q] = KG::dec_g(KG::load(static_cast<const TG*>(D.gA) +
+                                  ((uint32_t)q * D.qs + lvl_nbr<TG>(k, m, 0u, cz, (uint32_t)(cx + cy * (int)px), ps))));
+    else
+      X.g[q] = KG::dec_g(KG::load(static_cast<const TG*>(D.src_g[q]) + n));
   });
 }
 
@@ -396,7 +414,7 @@ __device__ __forceinline__ void moments_forces(const ParamsHead& P, const Column
 // secRelax + secCollision + secScalarCollision (kernel.js:308-386); writes the next state of cell n
 template <class S>
 __device__ __forceinline__ void collide_store(const DomainView& D, const ParamsHead& P,
-                                              const Column<RealOf<S>>& C, int k, uint32_t n,
+                                              const Column<RealOf<S>>& C, int k, uint32_t nf, uint32_t ng,
                                               const Cell<RealOf<S>>& X,
                                               const Macro<RealOf<S>>& M, uint32_t rs) {
   using R = RealOf<S>;
@@ -450,7 +468,7 @@ __device__ __forceinline__ void collide_store(const DomainView& D, const ParamsH
     const R fr = w45 * (qn - trN);
     const R cF = cdot<R, cx, cy, cz>(Fx, Fy, Fz);
     const R Fq = fpre * w * (R(3.0) * (cF - uF) + R(9.0) * cu * cF);
-    KF::store(fB + (n + D.plane[q]), enc_f_d<KF, q>(feq + om * fr + Fq, w, rs));
+    KF::store(fB + (nf + D.plane[q]), enc_f_d<KF, q>(feq + om * fr + Fq, w, rs));
   });
   R Ssrc = R(0);
   if (k == C.kg) Ssrc = R(C.qsrc) * R(P.srcscale);
@@ -460,7 +478,7 @@ __device__ __forceinline__ void collide_store(const DomainView& D, const ParamsH
     constexpr int cx = kC7[q][0], cy = kC7[q][1], cz = kC7[q][2];
     const R w = R(w7(q));
     const R geq = w * M.th * (R(1.0) + R(4.0) * cdot<R, cx, cy, cz>(ux, uy, uz));
-    KG::store(gB + (n + D.plane[q]), enc_g_d<KG, q>((X.g[q] + omg * (geq - X.g[q]) + w * Ssrc) * (R(1.0) - M.sg), rs));
+    KG::store(gB + (ng + D.plane[q]), enc_g_d<KG, q>((X.g[q] + omg * (geq - X.g[q]) + w * Ssrc) * (R(1.0) - M.sg), rs));
   });
 }
 
@@ -483,7 +501,7 @@ __device__ __forceinline__ double sponge_sg_d(const ParamsHead& P, int nz, int k
 // differs (held to the single-step theta rel-L2 <= 1e-5 bar).
 template <class S>
 __device__ __forceinline__ void fast_update(const DomainView& D, const ParamsHead& P, const RelaxConst& RK,
-                                            const Column<RealOf<S>>& C, int k, uint32_t n,
+                                            const Column<RealOf<S>>& C, int k, uint32_t nf, uint32_t ng,
                                             const Cell<RealOf<S>>& X,
                                             Macro<RealOf<S>>& M, uint32_t rs) {
   using R = RealOf<S>;
@@ -512,11 +530,11 @@ __device__ __forceinline__ void fast_update(const DomainView& D, const ParamsHea
       P, RK, m, X.g, X.uI, X.vI, X.kb, sg, Fx0, Fy0, Ssrc, tb_add, o,
       [&](auto Q, R x) {
         constexpr int q = Q;
-        KF::store(static_cast<StoreF<S>*>(D.dst_f[q]) + n, enc_f_x<KF, q>(x, R(w19(q)), rs));
+        KF::store(static_cast<StoreF<S>*>(D.dst_f[q]) + nf, enc_f_x<KF, q>(x, R(w19(q)), rs));
       },
       [&](auto Q, R v) {
         constexpr int q = Q;
-        KG::store(static_cast<StoreG<S>*>(D.dst_g[q]) + n, enc_g_d<KG, q>(v, rs));
+        KG::store(static_cast<StoreG<S>*>(D.dst_g[q]) + ng, enc_g_d<KG, q>(v, rs));
       });
   M.rho = m.rho;
   M.jx = m.jx;
@@ -589,24 +607,68 @@ __device__ __forceinline__ void pair_store_g(T* p, uint32_t ps, float2 v, uint32
   }
 }
 
+// The same for a level-paired 16-bit plane (lvl): the levels (k, k + 1), k even, of one population of a column are
+// one 32-bit word. Loads: the word at p holds both sources when the population has no vertical component (TWO =
+// false); else the sources are the high half of the word at p and the low half of the word one level pair up (p +
+// 2 ps), joined by one byte permutation. Decoded and encoded exactly as the single-cell codec does each half.
+template <bool TWO, class T>
+__device__ __forceinline__ uint32_t word_pull(const T* p, uint32_t ps) {
+  using K = Codec<T>;
+  const uint32_t a = K::load_w(p);
+  if constexpr (!TWO) return a;
+  else return __byte_perm(a, K::load_w(p + 2u * ps), 0x5432);
+}
+template <bool TWO, class T>
+__device__ __forceinline__ float2 word_load_f(const T* p, uint32_t ps, float w) {
+  using K = Codec<T>;
+  return vfma(K::raw2(word_pull<TWO>(p, ps)), vc<float2>(1.0 / K::kF), vc<float2>(w));
+}
+template <bool TWO, class T>
+__device__ __forceinline__ float2 word_load_g(const T* p, uint32_t ps) {
+  using K = Codec<T>;
+  return vmul(K::raw2(word_pull<TWO>(p, ps)), vc<float2>(1.0 / K::kG));
+}
+template <int P, class T>
+__device__ __forceinline__ void word_store_f(T* p, float2 x, float w, uint32_t h0, uint32_t h1) {
+  using K = Codec<T>;
+  const float sw = K::kF * w;
+  const float2 e = vfma(x, make_float2(sw, sw), make_float2(-sw, -sw));
+  if constexpr (K::kDither) K::store_w(p, K::cvt_sr2(e.x, e.y, h0 * kDitherMul<P>, h1 * kDitherMul<P>));
+  else K::store_w(p, K::cvt2(e.x, e.y));
+}
+template <int P, class T>
+__device__ __forceinline__ void word_store_g(T* p, float2 v, uint32_t h0, uint32_t h1) {
+  using K = Codec<T>;
+  const float2 e = vmul(v, vc<float2>(K::kG));
+  if constexpr (K::kDither) K::store_w(p, K::cvt_sr2(e.x, e.y, h0 * kDitherMul<19 + P>, h1 * kDitherMul<19 + P>));
+  else K::store_w(p, K::cvt2(e.x, e.y));
+}
+
 // Two vertically adjacent interior cells (k, k + 1) of one column, streamed and relaxed as the two lanes of packed
-// f32x2 arithmetic. Interior cells are never the first fluid cell (no drag, no source); the result of each lane is
-// bit-identical to stream_interior + fast_update on that cell alone.
+// f32x2 arithmetic (mc = j px + i; k even when a population plane is level-paired: then each population of the two
+// cells is one word). Interior cells are never the first fluid cell (no drag, no source); the result of each lane is bit-identical
+// to stream_interior + fast_update on that cell alone.
 template <class S>
 __device__ __forceinline__ void fast_pair(const DomainView& D, const ParamsHead& P, const RelaxConst& RK,
-                                          const float4* prof, const Column<float>& C, int k, uint32_t n, uint32_t r0,
+                                          const float4* prof, const Column<float>& C, int k, uint32_t mc, uint32_t r0,
                                           uint32_t r1) {
-  StoreF<S>* fB = static_cast<StoreF<S>*>(D.fB);
-  StoreG<S>* gB = static_cast<StoreG<S>*>(D.gB);
+  using TF = StoreF<S>;
+  using TG = StoreG<S>;
   const uint32_t ps = D.ps;
+  // own element offsets: the pair's word in a level-paired plane (lvl of the even level k), else level k's cell
+  const uint32_t nf = lvl<TF>(k, mc, ps), ng = lvl<TG>(k, mc, ps);
   float2 f[19], g[7];
   static_for<19>([&](auto Q) {
     constexpr int q = Q;
-    f[q] = pair_load_f(static_cast<const StoreF<S>*>(D.src_f[q]) + n, ps, (float)w19(q));
+    const TF* src = static_cast<const TF*>(D.src_f[q]) + nf;
+    if constexpr (kLevelPairs<TF>) f[q] = word_load_f<kC19[q][2] != 0>(src, ps, (float)w19(q));
+    else f[q] = pair_load_f(src, ps, (float)w19(q));
   });
   static_for<7>([&](auto Q) {
     constexpr int q = Q;
-    g[q] = pair_load_g(static_cast<const StoreG<S>*>(D.src_g[q]) + n, ps);
+    const TG* src = static_cast<const TG*>(D.src_g[q]) + ng;
+    if constexpr (kLevelPairs<TG>) g[q] = word_load_g<kC7[q][2] != 0>(src, ps);
+    else g[q] = pair_load_g(src, ps);
   });
   const int z0 = min(max(k - C.ktc, 0), D.nz - 1), z1 = min(max(k + 1 - C.ktc, 0), D.nz - 1);
   const float4 p0 = prof[z0], p1 = prof[z1];
@@ -620,11 +682,15 @@ __device__ __forceinline__ void fast_pair(const DomainView& D, const ParamsHead&
       make_float2(sponge_sg(P, D.nz, k), sponge_sg(P, D.nz, k + 1)), zero, zero, zero, tb_add, o,
       [&](auto Q, float2 v) {
         constexpr int q = Q;
-        pair_store_f<q>(static_cast<StoreF<S>*>(D.dst_f[q]) + n, ps, v, (float)w19(q), r0, r1);
+        TF* dst = static_cast<TF*>(D.dst_f[q]) + nf;
+        if constexpr (kLevelPairs<TF>) word_store_f<q>(dst, v, (float)w19(q), r0, r1);
+        else pair_store_f<q>(dst, ps, v, (float)w19(q), r0, r1);
       },
       [&](auto Q, float2 v) {
         constexpr int q = Q;
-        pair_store_g<q>(static_cast<StoreG<S>*>(D.dst_g[q]) + n, ps, v, r0, r1);
+        TG* dst = static_cast<TG*>(D.dst_g[q]) + ng;
+        if constexpr (kLevelPairs<TG>) word_store_g<q>(dst, v, r0, r1);
+        else pair_store_g<q>(dst, ps, v, r0, r1);
       });
 }
 
@@ -653,7 +719,10 @@ __device__ __forceinline__ void prefetch_level(const DomainView& D, int k, uint3
   const int cz = (int)((kZp >> lane) & 1u) - (int)((kZn >> lane) & 1u);
   const bool isf = lane < 19;
   const int q = isf ? lane : lane - 19;
-  const int64_t n = (int64_t)q * D.qs + (int64_t)(k - cz) * D.ps + (int64_t)rowbase - (int64_t)cy * D.px;
+  const int64_t mrow = (int64_t)rowbase - (int64_t)cy * D.px;
+  const bool lp = isf ? kLevelPairs<StoreF<S>> : kLevelPairs<StoreG<S>>;
+  const int64_t n = (int64_t)q * D.qs + (lp ? (int64_t)((k - cz) >> 1) * 2 * D.ps + 2 * mrow
+                                            : (int64_t)(k - cz) * D.ps + mrow);
   const int64_t lim = (int64_t)(isf ? 19 : 7) * D.qs - 64;
   const int64_t e = n < 0 ? 0 : (n > lim ? lim : n);
   const char* p = isf ? static_cast<const char*>(D.fA) + e * (int64_t)sizeof(StoreF<S>)
@@ -732,6 +801,8 @@ __device__ __forceinline__ void step_block(const DomainView& D, int bx, int by, 
   // PAIRS (FMA build without output modes): two interior levels at a time on the packed f32x2 lanes when every
   // active lane of the warp has both cells interior (bit-identical to the single-level path; more registers)
   constexpr bool kPairs = PAIRS && FAST && MODE == 0 && !BUDGET && std::is_same_v<R, float>;
+  // a level-paired plane pairs the levels (2t, 2t + 1) only: an odd first level runs alone
+  constexpr bool kEvenPairs = kLevelPairs<StoreF<S>> || kLevelPairs<StoreG<S>>;
   // FMA build, plain steps, launch option: the next level's (pair's) source rows are prefetched into L2 one level
   // (pair) ahead
   constexpr bool kPrefetch = FAST && MODE == 0 && !BUDGET;   // (main blocks only: strip lanes are not one row)
@@ -745,11 +816,11 @@ __device__ __forceinline__ void step_block(const DomainView& D, int bx, int by, 
       }
     }
     if constexpr (kPairs) {
-      if (k + 1 < k1) {
+      if (k + 1 < k1 && (!kEvenPairs || (k & 1) == 0)) {
         const bool in2 = valid && k >= C.kg && !C.face && k >= C.kint && k + 1 < D.nz - 1;
         const unsigned m2 = __ballot_sync(0xffffffffu, valid && k + 1 >= C.kg);
         if (m2 != 0u && __ballot_sync(0xffffffffu, in2) == m2) {
-          if (in2) fast_pair<S>(D, P, RK, smem_prof, C, k, (uint32_t)k * D.ps + base, seed(k), seed(k + 1));
+          if (in2) fast_pair<S>(D, P, RK, smem_prof, C, k, base, seed(k), seed(k + 1));
           ++k;
           continue;
         }
@@ -760,16 +831,17 @@ __device__ __forceinline__ void step_block(const DomainView& D, int bx, int by, 
     const bool inter = act && !C.face && k >= C.kint && k < D.nz - 1;
     const bool all_inter = __ballot_sync(0xffffffffu, inter) == m;
     if (act) {
-      const uint32_t n = (uint32_t)k * D.ps + base;
+      const uint32_t n = (uint32_t)k * D.ps + base;   // the cell in [k][j][px] order (output modes)
+      const uint32_t nf = lvl<StoreF<S>>(k, base, D.ps), ng = lvl<StoreG<S>>(k, base, D.ps);
       Cell<R> X;
-      if (all_inter) stream_interior<S>(D, smem_prof, C, k, n, X);
-      else stream_cell<S>(D, P, smem_prof, C, k, n, X);
+      if (all_inter) stream_interior<S>(D, smem_prof, C, k, base, X);
+      else stream_cell<S>(D, P, smem_prof, C, k, base, X);
       Macro<R> M;
       if constexpr (FAST) {
-        fast_update<S>(D, P, RK, C, k, n, X, M, seed(k));
+        fast_update<S>(D, P, RK, C, k, nf, ng, X, M, seed(k));
       } else {
         moments_forces<R>(P, C, k, D.nz, X, M);
-        collide_store<S>(D, P, C, k, n, X, M, seed(k));
+        collide_store<S>(D, P, C, k, nf, ng, X, M, seed(k));
       }
       if constexpr (MODE == 1) {
         D.dbg[n] = make_float4((float)M.th, (float)M.ux, (float)M.uy, (float)M.uz);

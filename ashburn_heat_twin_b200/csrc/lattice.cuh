@@ -112,6 +112,17 @@ struct Codec<__half> {
   static constexpr float kF = kScaleF16, kG = kScaleG16;
   __device__ __forceinline__ static float raw(__half v) { return __half2float(v); }
   __device__ __forceinline__ static __half cvt(float v) { return __float2half_rn(v); }
+  // a level-pair word (low half: the even level): load, store, both halves widened, two values narrowed
+  __device__ __forceinline__ static uint32_t load_w(const __half* p) { return __ldg(reinterpret_cast<const unsigned*>(p)); }
+  __device__ __forceinline__ static void store_w(__half* p, uint32_t w) { __stcs(reinterpret_cast<unsigned*>(p), w); }
+  __device__ __forceinline__ static float2 raw2(uint32_t w) {
+    return make_float2(__half2float(__ushort_as_half((unsigned short)(w & 0xFFFFu))),
+                       __half2float(__ushort_as_half((unsigned short)(w >> 16))));
+  }
+  __device__ __forceinline__ static uint32_t cvt2(float lo, float hi) {
+    const __half2 h = __floats2half2_rn(lo, hi);
+    return *reinterpret_cast<const uint32_t*>(&h);
+  }
 };
 
 template <>
@@ -141,6 +152,20 @@ struct Codec<__nv_bfloat16> {
   static constexpr float kF = kScaleBF16, kG = kScaleBF16;
   __device__ __forceinline__ static float raw(__nv_bfloat16 v) { return __bfloat162float(v); }
   __device__ __forceinline__ static __nv_bfloat16 cvt(float v) { return __float2bfloat16_rn(v); }
+  __device__ __forceinline__ static uint32_t load_w(const __nv_bfloat16* p) {
+    return __ldg(reinterpret_cast<const unsigned*>(p));
+  }
+  __device__ __forceinline__ static void store_w(__nv_bfloat16* p, uint32_t w) {
+    __stcs(reinterpret_cast<unsigned*>(p), w);
+  }
+  // a BF16 value is the high half of its f32 (exact widening)
+  __device__ __forceinline__ static float2 raw2(uint32_t w) {
+    return make_float2(__uint_as_float(w << 16), __uint_as_float(w & 0xFFFF0000u));
+  }
+  __device__ __forceinline__ static uint32_t cvt2(float lo, float hi) {
+    const __nv_bfloat162 h = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<const uint32_t*>(&h);
+  }
 };
 
 // FP16 storage whose step stores round stochastically: the same bits in memory as the __half codec ((f - w) * 16
@@ -184,6 +209,12 @@ struct Codec<half_sr> {
   }
   __device__ __forceinline__ static void store_bits(half_sr* p, uint32_t b16) {
     __stcs(reinterpret_cast<unsigned short*>(p), (unsigned short)b16);
+  }
+  __device__ __forceinline__ static uint32_t load_w(const half_sr* p) { return __ldg(reinterpret_cast<const unsigned*>(p)); }
+  __device__ __forceinline__ static void store_w(half_sr* p, uint32_t w) { __stcs(reinterpret_cast<unsigned*>(p), w); }
+  __device__ __forceinline__ static float2 raw2(uint32_t w) {
+    return make_float2(__half2float(__ushort_as_half((unsigned short)(w & 0xFFFFu))),
+                       __half2float(__ushort_as_half((unsigned short)(w >> 16))));
   }
   __device__ __forceinline__ static float dec_f(half_sr v, float w) { return __fmaf_rn(raw(v), 1.0f / kScaleF16, w); }
   __device__ __forceinline__ static float dec_g(half_sr v) { return __fmul_rn(raw(v), 1.0f / kScaleG16); }
@@ -237,6 +268,27 @@ template <class K, int P, class R>
 __device__ __forceinline__ auto enc_g_d(R v, uint32_t h) {
   if constexpr (K::kDither) return K::enc_g_sr(v, h * kDitherMul<19 + P>);
   else return K::enc_g(v);
+}
+
+// Population layout in HBM. A population plane holds the levels of px x ny pitched rows (m = j px + i in a level).
+// 32- and 64-bit elements keep each level as its own plane: element k ps + m. 16-bit elements keep the two levels of
+// a pair (2t, 2t + 1) side by side in one 32-bit word: element t (2 ps) + 2 m + (k & 1), so the paired step loads and
+// stores both levels of a column with one 32-bit access (a plane then holds nz rounded up to even levels).
+template <class T>
+inline constexpr bool kLevelPairs = sizeof(T) == 2;
+// element offset of level k, row-column m in a population plane; unsigned arithmetic, so a neighbour offset that
+// steps below 0 wraps and comes back when the population plane's offset is added
+template <class T>
+__host__ __device__ __forceinline__ uint32_t lvl(int k, uint32_t m, uint32_t ps) {
+  if constexpr (kLevelPairs<T>) return (uint32_t)(k >> 1) * (2u * ps) + 2u * m + (uint32_t)(k & 1);
+  else return (uint32_t)k * ps + m;
+}
+
+// element offset of the neighbour (k - cz, m - d) of the cell (k, m) whose own offset is n (= lvl<T>(k, m, ps))
+template <class T>
+__host__ __device__ __forceinline__ uint32_t lvl_nbr(int k, uint32_t m, uint32_t n, int cz, uint32_t d, uint32_t ps) {
+  if constexpr (kLevelPairs<T>) return lvl<T>(k - cz, m - d, ps);
+  else return n - (d + (uint32_t)(cz * (int)ps));
 }
 
 // Storage of a state: a plain type stores f and g alike; Mixed<SF, SG> stores the flow populations f as SF and the
@@ -306,10 +358,11 @@ struct DomainView {
   int jg0, nyg, jlo, jhi;
   int jbase;                    // first local row the launch's grid covers (0 unless a step of a band of rows)
   int strip;                    // strip width of the column split (step_split)
-  uint32_t ps;                  // plane stride px*ny
-  uint32_t qs;                  // q stride px*ny*nz
-  // element offset of the interior pull source of population q relative to the cell: q*qs - (cx + cy*px + cz*ps)
-  // (kernel-parameter table, so each gather is one add of a constant operand)
+  uint32_t ps;                  // level stride px*ny (a 16-bit plane's level pair: 2 ps, lvl)
+  uint32_t qs;                  // population plane stride: ps x (nz, rounded up to even with a 16-bit population)
+  // element offset of the interior pull source of population q relative to the cell: q*qs - (cx + cy*px + cz*ps);
+  // level-paired planes: of the first source word of a level pair (pull_offset). Kernel-parameter tables, so each
+  // gather is one add of a constant operand
   uint32_t pull_f[19], pull_g[7];
   uint32_t plane[19];           // q*qs
   // interior accesses as (base pointer + cell index): the pull source of each population (fA / gA + pull offset) and
@@ -320,14 +373,22 @@ struct DomainView {
   void* dst_g[7];
 };
 
-// fill the offset tables of a view from its strides
-inline void set_offsets(DomainView& D) {   // host only
+// pull offset of population q with velocity (cx, cy, cz) for one storage element size (host only): the element offset
+// of the interior pull source relative to the cell. Level-paired 16-bit planes (esize 2): the offset of the first of
+// the source words of a level pair (2t, 2t + 1) relative to the pair's word: the pair's sources are levels 2t - cz and
+// 2t + 1 - cz, in one word for cz = 0, else in this word and the next one up (2 ps further).
+inline uint32_t pull_offset(int esize, uint32_t qs, uint32_t px, uint32_t ps, int q, int cx, int cy, int cz) {
+  if (esize == 2) return (uint32_t)q * qs - 2u * (uint32_t)(cx + cy * (int)px) - (cz == 1 ? 2u * ps : 0u);
+  return (uint32_t)q * qs - (uint32_t)(cx + cy * (int)px + cz * (int)ps);
+}
+
+// fill the offset tables of a view from its strides and element sizes (host only)
+inline void set_offsets(DomainView& D, int esize_f, int esize_g) {
   for (int q = 0; q < 19; ++q) {
     D.plane[q] = (uint32_t)q * D.qs;
-    D.pull_f[q] = (uint32_t)q * D.qs - (uint32_t)(kC19[q][0] + kC19[q][1] * D.px + kC19[q][2] * (int)D.ps);
+    D.pull_f[q] = pull_offset(esize_f, D.qs, (uint32_t)D.px, D.ps, q, kC19[q][0], kC19[q][1], kC19[q][2]);
   }
-  for (int q = 0; q < 7; ++q)
-    D.pull_g[q] = (uint32_t)q * D.qs - (uint32_t)(kC7[q][0] + kC7[q][1] * D.px + kC7[q][2] * (int)D.ps);
+  for (int q = 0; q < 7; ++q) D.pull_g[q] = pull_offset(esize_g, D.qs, (uint32_t)D.px, D.ps, q, kC7[q][0], kC7[q][1], kC7[q][2]);
 }
 
 // fill the interior base pointers of a view from its state pointers and offset tables (host only; call again when

@@ -155,8 +155,10 @@ static cudaError_t launch_tma(const DomainView& D, const StepLaunch& L, cudaStre
 
 template <class S, int MODE, bool BUDGET>
 static cudaError_t launch_t(const DomainView& D, const StepLaunch& L, cudaStream_t s) {
-  if constexpr (MODE == 0 && !BUDGET && std::is_same_v<StoreF<S>, StoreG<S>> && !kDitherOf<S>) {
-    // the staged kernel stages f and g with one element size: uniform round-to-nearest storages only
+  if constexpr (MODE == 0 && !BUDGET && std::is_same_v<StoreF<S>, StoreG<S>> && !kDitherOf<S> &&
+                !kLevelPairs<StoreF<S>>) {
+    // the staged kernel stages f and g with one element size, one level per box: uniform round-to-nearest storages
+    // of 4- and 8-byte elements only
     if (L.tma_ty > 0 && L.maps != nullptr) return launch_tma<S>(D, L, s);
   }
   const int minb = (MODE == 0 && !BUDGET) ? L.minb : 0;

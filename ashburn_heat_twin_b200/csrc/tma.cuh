@@ -162,6 +162,8 @@ constexpr size_t tma_smem_bytes(int nz) {
 template <class S, bool FAST, int TY, int DEPTH>
 __device__ __forceinline__ void step_tma_block(const DomainView& D, const TmaMaps& M, int zslab) {
   static_assert(!kDitherOf<S>, "the staged kernel takes no dither (stochastic-rounding storages use the plain kernel)");
+  static_assert(!kLevelPairs<StoreF<S>>, "the staged kernel's boxes are single levels (level-paired planes use the plain "
+                                         "kernel)");
   using R = typename Codec<S>::Real;
   using G = TmaGeom<S>;
   constexpr int STAGE = G::template stage_bytes<TY>();
@@ -225,14 +227,14 @@ __device__ __forceinline__ void step_tma_block(const DomainView& D, const TmaMap
         X.kb = R(pr.z);
         stage_read<S, TY>(stage, tx, ty, X);
       } else {
-        stream_cell<S>(D, P, prof, C, k, n, X);
+        stream_cell<S>(D, P, prof, C, k, cbase, X);
       }
       Macro<R> Mc;
       if constexpr (FAST) {
-        fast_update<S>(D, P, RK, C, k, n, X, Mc, 0u);
+        fast_update<S>(D, P, RK, C, k, n, n, X, Mc, 0u);
       } else {
         moments_forces<R>(P, C, k, D.nz, X, Mc);
-        collide_store<S>(D, P, C, k, n, X, Mc, 0u);
+        collide_store<S>(D, P, C, k, n, n, X, Mc, 0u);
       }
     }
     __syncthreads();   // stage s consumed by every thread
