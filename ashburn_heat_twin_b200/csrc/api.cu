@@ -115,10 +115,16 @@ StepLaunch ahx::solo_launch(const ahx_handle* h, int parity) {
   L.zslab = h->zslab;
   L.minb = h->minb;
   L.pairs = h->pairs;
-  L.tma_ty = h->maps_ok ? h->tma_ty : 0;
+  L.tma_ty = (h->pairs ? h->pmaps_ok : h->maps_ok) ? h->tma_ty : 0;
   L.tma_depth = h->tma_depth;
-  L.maps = L.tma_ty ? &h->maps[L.tma_ty == 8 ? 1 : 0][parity] : nullptr;
+  L.maps = stage_maps(h, L, parity);
   return L;
+}
+
+const TmaMaps* ahx::stage_maps(const ahx_handle* h, const StepLaunch& L, int parity) {
+  if (!L.tma_ty) return nullptr;
+  const int t = L.tma_ty == 8 ? 1 : 0;
+  return L.pairs ? &h->pmaps[t][parity] : &h->maps[t][parity];
 }
 
 uint64_t ahx::solo_launch_key(const ahx_handle* h) {
@@ -177,6 +183,28 @@ bool make_maps(ahx_handle* h, void* f, void* g, int ty, TmaMaps* M) {
   const int H = 16 / h->esize;
   return encode_map(h, f, 19, 32 + 2 * H, ty, &M->fw) && encode_map(h, f, 19, 32, ty, &M->fn) &&
          encode_map(h, g, 7, 32 + 2 * H, ty, &M->gw) && encode_map(h, g, 7, 32, ty, &M->gn);
+}
+
+// 4-D tensor map [q][level pair][y][x] of 32-bit words over a level-paired 16-bit population buffer (word (t, j, i)
+// holds the levels 2t and 2t + 1 of column (i, j)), with a box of width x TY x 1 x 1 words
+bool encode_pair_map(ahx_handle* h, void* buf, int nq, int width, int ty, CUtensorMap* out) {
+  EncodeTiledFn fn = encode_fn();
+  if (!fn) return false;
+  const cuuint64_t dims[4] = {(cuuint64_t)h->dims.nx, (cuuint64_t)h->dims.ny, (cuuint64_t)((h->dims.nz + 1) / 2),
+                              (cuuint64_t)nq};
+  // row: px words; level pair: ps words; population plane: qs 16-bit elements
+  const cuuint64_t strides[3] = {(cuuint64_t)h->px * 4, (cuuint64_t)h->ps * 4, (cuuint64_t)h->qs * 2};
+  const cuuint32_t box[4] = {(cuuint32_t)width, (cuuint32_t)ty, 1, 1};
+  const cuuint32_t estr[4] = {1, 1, 1, 1};
+  return fn(out, CU_TENSOR_MAP_DATA_TYPE_UINT32, 4, buf, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+            CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// the four word maps of a level-paired state for the staged paired step (wide boxes: 4 words of halo on each side)
+bool make_pair_maps(ahx_handle* h, void* f, void* g, int ty, TmaMaps* M) {
+  return encode_pair_map(h, f, 19, 40, ty, &M->fw) && encode_pair_map(h, f, 19, 32, ty, &M->fn) &&
+         encode_pair_map(h, g, 7, 40, ty, &M->gw) && encode_pair_map(h, g, 7, 32, ty, &M->gn);
 }
 
 // a staged copy that ran out of time leaves its block's cells unstepped: report it (the state is not usable)
@@ -366,6 +394,11 @@ ahx_status ahx_create(const ahx_dims* dims, ahx_handle** out) {
   h->maps_ok = h->esize == h->esize_g && h->esize != 2 && dims->precision != AHX_FP16_SR;
   for (int t = 0; t < 2 && h->maps_ok; ++t)
     for (int p = 0; p < 2; ++p) h->maps_ok = h->maps_ok && make_maps(h, h->f[p], h->g[p], t ? 8 : 4, &h->maps[t][p]);
+  // the staged paired step reads level-paired f and g (the 16-bit storages)
+  h->pmaps_ok = h->esize == 2 && h->esize_g == 2;
+  for (int t = 0; t < 2 && h->pmaps_ok; ++t)
+    for (int p = 0; p < 2; ++p)
+      h->pmaps_ok = h->pmaps_ok && make_pair_maps(h, h->f[p], h->g[p], t ? 8 : 4, &h->pmaps[t][p]);
   cudaMemsetAsync(h->d_params, 0, 64 + 16 * (size_t)dims->nz, h->s_step);
   cudaMemsetAsync(h->d_colv, 0, NXY * sizeof(uint4), h->s_step);
   cudaMemsetAsync(h->d_ktop, 0, NXY * 4, h->s_step);
@@ -556,7 +589,7 @@ ahx_status ahx_step(ahx_handle* h, int n, int mode) {
   }
   for (; s < n; ++s) {
     L.mode = (mode == AHX_MODE_ACC) ? 2 : ((mode == AHX_MODE_OUT && s == n - 1) ? 1 : 0);
-    L.maps = L.tma_ty ? &h->maps[L.tma_ty == 8 ? 1 : 0][h->parity] : nullptr;
+    L.maps = stage_maps(h, L, h->parity);
     DomainView D = view(h);
     const cudaError_t e = h->dims.arith == AHX_ARITH_FAST ? fast::launch_step(D, L, h->s_step)
                                                             : exact::launch_step(D, L, h->s_step);
@@ -933,8 +966,9 @@ ahx_status ahx_set_slab(ahx_handle* h, int jg0, int nyg, int jlo, int jhi) {
   h->nyg = nyg;
   h->jlo = jlo;
   h->jhi = jhi;
-  // the staged kernel updates whole row blocks: slabs use the plain kernels
+  // the staged kernels update whole row blocks: slabs use the plain kernels
   h->maps_ok = false;
+  h->pmaps_ok = false;
   h->tma_ty = h->tma_depth = 0;
   return AHX_OK;
 }
@@ -1036,12 +1070,28 @@ ahx_status ahx_set_launch(ahx_handle* h, int block_y, int zslab) {
       return fail(AHX_EINVAL, "live solver: paired levels need the FMA build and f32 arithmetic");
     block_y -= 2000;
   }
-  if (block_y >= 1000) {   // staged kernel: 1000 + 100 x depth + rows (4 with depth 2-4, or 8 with depth 2-3)
+  if (block_y >= 1000 && pairs) {
+    // staged paired step of the 16-bit storages: 2000 + 1000 + 100 x depth + rows (4 with depth 2-4, or 8 with
+    // depth 2-3)
+    const int ty = block_y % 100, dp = (block_y / 100) % 10;
+    if (!((ty == 4 && dp >= 2 && dp <= 4) || (ty == 8 && dp >= 2 && dp <= 3)) || zslab < 0)
+      return fail(AHX_EINVAL, "live solver: bad staged paired launch shape");
+    if (!h->pmaps_ok)
+      return fail(AHX_EINVAL, "live solver: the staged paired step needs a whole-domain 16-bit state (FP16, BF16 or "
+                              "FP16 with stochastic rounding)");
+    if (pf) return fail(AHX_EINVAL, "live solver: the staged paired step has no prefetch variant");
+    h->tma_ty = ty;
+    h->tma_depth = dp;
+    h->block_y = ty;
+    h->minb = 0;
+    h->pairs = true;
+    h->prefetch = false;
+  } else if (block_y >= 1000) {   // staged kernel: 1000 + 100 x depth + rows (4 with depth 2-4, or 8 with depth 2-3)
     const int ty = block_y % 100, dp = (block_y / 100) % 10;
     if (!((ty == 4 && dp >= 2 && dp <= 4) || (ty == 8 && dp >= 2 && dp <= 3)) || zslab < 0)
       return fail(AHX_EINVAL, "live solver: bad staged launch shape");
     if (!h->maps_ok) return fail(AHX_EINVAL, "live solver: tensor maps unavailable for the staged kernel");
-    if (pairs || pf) return fail(AHX_EINVAL, "live solver: the staged kernel has no paired or prefetch variant");
+    if (pf) return fail(AHX_EINVAL, "live solver: the staged kernel has no prefetch variant");
     h->tma_ty = ty;
     h->tma_depth = dp;
     h->block_y = ty;
@@ -1099,9 +1149,11 @@ ahx_status ahx_autotune(ahx_handle* h, int steps_per_trial, int* best_block_y, i
     for (Shape sh : {Shape{4, 4, 0, 0, true}, Shape{4, 5, 0, 0, true}, Shape{4, 6, 0, 0, true},
                      Shape{4, 8, 0, 0, true}})
       shapes.push_back(sh);
-  // The TMA-staged kernel is not a candidate: it never won a trial (16-20 against 26.6 GLUPS on 600x600x64) and an
-  // early build of it once stopped with a misaligned-address error whose cause was not found. It stays reachable only
-  // through an explicit ahx_set_launch value.
+  // The TMA-staged kernels are not candidates. The single-level one never won a trial (16-20 against 26.6 GLUPS on
+  // 600x600x64) and an early build of it once stopped with a misaligned-address error whose cause was not found; the
+  // staged paired step of the 16-bit storages runs 27.6-29.1 against 36.1 GLUPS for the plain paired step there (half
+  // the resident warps, a block barrier per level pair). Both stay reachable only through explicit ahx_set_launch
+  // values.
   // thin slabs put more blocks in flight on small grids, where one 6-level wave leaves the SMs latency-bound
   std::vector<int> zss = {h->dims.nz, 32, 16, 12, 8, 6, 4, 3, 2};
   DomainView D = view(h);
@@ -1212,9 +1264,10 @@ ahx_status ahx_autotune(ahx_handle* h, int steps_per_trial, int* best_block_y, i
   h->pairs = bpr;
   h->prefetch = bpf != 0;
   // the ahx_set_launch encoding: variant x 100 + block_y (+ 2000 for paired levels, + 10000 for the L2 prefetch),
-  // or 1000 + 100 x depth + rows for the staged kernel
+  // or 1000 + 100 x depth + rows for a staged kernel (+ 2000 for the staged paired step)
   if (best_block_y)
-    *best_block_y = bty ? 1000 + 100 * bdp + bty : (bpf ? 10000 : 0) + (bpr ? 2000 : 0) + bmb * 100 + bby;
+    *best_block_y = bty ? (bpr ? 2000 : 0) + 1000 + 100 * bdp + bty
+                        : (bpf ? 10000 : 0) + (bpr ? 2000 : 0) + bmb * 100 + bby;
   if (best_zslab) *best_zslab = bzs;
   if (best_ms) *best_ms = best;
   return AHX_OK;

@@ -618,15 +618,24 @@ __device__ __forceinline__ uint32_t word_pull(const T* p, uint32_t ps) {
   if constexpr (!TWO) return a;
   else return __byte_perm(a, K::load_w(p + 2u * ps), 0x5432);
 }
+// both halves of a level-pair word decoded (flow: h / s + w; temperature: h / s)
+template <class T>
+__device__ __forceinline__ float2 word_dec_f(uint32_t wd, float w) {
+  using K = Codec<T>;
+  return vfma(K::raw2(wd), vc<float2>(1.0 / K::kF), vc<float2>(w));
+}
+template <class T>
+__device__ __forceinline__ float2 word_dec_g(uint32_t wd) {
+  using K = Codec<T>;
+  return vmul(K::raw2(wd), vc<float2>(1.0 / K::kG));
+}
 template <bool TWO, class T>
 __device__ __forceinline__ float2 word_load_f(const T* p, uint32_t ps, float w) {
-  using K = Codec<T>;
-  return vfma(K::raw2(word_pull<TWO>(p, ps)), vc<float2>(1.0 / K::kF), vc<float2>(w));
+  return word_dec_f<T>(word_pull<TWO>(p, ps), w);
 }
 template <bool TWO, class T>
 __device__ __forceinline__ float2 word_load_g(const T* p, uint32_t ps) {
-  using K = Codec<T>;
-  return vmul(K::raw2(word_pull<TWO>(p, ps)), vc<float2>(1.0 / K::kG));
+  return word_dec_g<T>(word_pull<TWO>(p, ps));
 }
 template <int P, class T>
 __device__ __forceinline__ void word_store_f(T* p, float2 x, float w, uint32_t h0, uint32_t h1) {
@@ -642,6 +651,41 @@ __device__ __forceinline__ void word_store_g(T* p, float2 v, uint32_t h0, uint32
   const float2 e = vmul(v, vc<float2>(K::kG));
   if constexpr (K::kDither) K::store_w(p, K::cvt_sr2(e.x, e.y, h0 * kDitherMul<19 + P>, h1 * kDitherMul<19 + P>));
   else K::store_w(p, K::cvt2(e.x, e.y));
+}
+
+// The relaxation and the stores of an interior cell pair (k, k + 1) of one column (fast_pair below, and the TMA-staged
+// paired step), given the decoded pull sources of both cells as the two lanes of each population (nf, ng: the pair's
+// own element offsets).
+template <class S>
+__device__ __forceinline__ void fast_pair_relax(const DomainView& D, const ParamsHead& P, const RelaxConst& RK,
+                                                const float4* prof, const Column<float>& C, int k, uint32_t nf,
+                                                uint32_t ng, const float2 (&f)[19], const float2 (&g)[7], uint32_t r0,
+                                                uint32_t r1) {
+  using TF = StoreF<S>;
+  using TG = StoreG<S>;
+  const uint32_t ps = D.ps;
+  const int z0 = min(max(k - C.ktc, 0), D.nz - 1), z1 = min(max(k + 1 - C.ktc, 0), D.nz - 1);
+  const float4 p0 = prof[z0], p1 = prof[z1];
+  Moments<float2> m;
+  lane_moments<float2>(f, g, m);
+  const float2 zero = vc<float2>(0.0);
+  const float2 tb_add = C.spon ? vc<float2>(C.spg) : zero;
+  Relaxed<float2> o;
+  lane_relax<float2>(
+      P, RK, m, g, make_float2(p0.x, p1.x), make_float2(p0.y, p1.y), make_float2(p0.z, p1.z),
+      make_float2(sponge_sg(P, D.nz, k), sponge_sg(P, D.nz, k + 1)), zero, zero, zero, tb_add, o,
+      [&](auto Q, float2 v) {
+        constexpr int q = Q;
+        TF* dst = static_cast<TF*>(D.dst_f[q]) + nf;
+        if constexpr (kLevelPairs<TF>) word_store_f<q>(dst, v, (float)w19(q), r0, r1);
+        else pair_store_f<q>(dst, ps, v, (float)w19(q), r0, r1);
+      },
+      [&](auto Q, float2 v) {
+        constexpr int q = Q;
+        TG* dst = static_cast<TG*>(D.dst_g[q]) + ng;
+        if constexpr (kLevelPairs<TG>) word_store_g<q>(dst, v, r0, r1);
+        else pair_store_g<q>(dst, ps, v, r0, r1);
+      });
 }
 
 // Two vertically adjacent interior cells (k, k + 1) of one column, streamed and relaxed as the two lanes of packed
@@ -670,28 +714,7 @@ __device__ __forceinline__ void fast_pair(const DomainView& D, const ParamsHead&
     if constexpr (kLevelPairs<TG>) g[q] = word_load_g<kC7[q][2] != 0>(src, ps);
     else g[q] = pair_load_g(src, ps);
   });
-  const int z0 = min(max(k - C.ktc, 0), D.nz - 1), z1 = min(max(k + 1 - C.ktc, 0), D.nz - 1);
-  const float4 p0 = prof[z0], p1 = prof[z1];
-  Moments<float2> m;
-  lane_moments<float2>(f, g, m);
-  const float2 zero = vc<float2>(0.0);
-  const float2 tb_add = C.spon ? vc<float2>(C.spg) : zero;
-  Relaxed<float2> o;
-  lane_relax<float2>(
-      P, RK, m, g, make_float2(p0.x, p1.x), make_float2(p0.y, p1.y), make_float2(p0.z, p1.z),
-      make_float2(sponge_sg(P, D.nz, k), sponge_sg(P, D.nz, k + 1)), zero, zero, zero, tb_add, o,
-      [&](auto Q, float2 v) {
-        constexpr int q = Q;
-        TF* dst = static_cast<TF*>(D.dst_f[q]) + nf;
-        if constexpr (kLevelPairs<TF>) word_store_f<q>(dst, v, (float)w19(q), r0, r1);
-        else pair_store_f<q>(dst, ps, v, (float)w19(q), r0, r1);
-      },
-      [&](auto Q, float2 v) {
-        constexpr int q = Q;
-        TG* dst = static_cast<TG*>(D.dst_g[q]) + ng;
-        if constexpr (kLevelPairs<TG>) word_store_g<q>(dst, v, r0, r1);
-        else pair_store_g<q>(dst, ps, v, r0, r1);
-      });
+  fast_pair_relax<S>(D, P, RK, prof, C, k, nf, ng, f, g, r0, r1);
 }
 
 // Population slot p of a cell update: f population p (p < 19) or g population p - 19 (p < 26). Bit p of these masks

@@ -79,6 +79,8 @@ struct ahx_handle {
   int tma_ty = 0, tma_depth = 0;          // staged kernel selected when tma_ty > 0
   bool maps_ok = false;
   ahx::TmaMaps maps[2][2];                     // [TY 4 / 8][parity]: tensor maps of the state read by a step
+  bool pmaps_ok = false;
+  ahx::TmaMaps pmaps[2][2];                    // the same over the 32-bit words of level-paired 16-bit planes
   int* d_err = nullptr;                   // error word the staged kernel sets
   bool prefetch = false;                  // next-level L2 prefetch in the step (launch option, FMA build)
   uint32_t* d_tick = nullptr;             // step counter pair of the stochastic-rounding storage, then the tuner's
@@ -103,6 +105,8 @@ ahx_status check(ahx_handle* h);                                             // 
 DomainView view_at(ahx_handle* h, int parity);                               // the state read at this parity
 StepLaunch solo_launch(const ahx_handle* h, int parity);   // a plain step of this handle (its launch shape) at a parity
 uint64_t solo_launch_key(const ahx_handle* h);             // everything solo_launch depends on besides the parity
+// the tensor maps a staged launch reads at a parity (single-level or paired-word maps), or null for a plain launch
+const TmaMaps* stage_maps(const ahx_handle* h, const StepLaunch& L, int parity);
 cudaError_t solo_step(ahx_handle* h, int parity, cudaStream_t s);   // launch one plain step reading that parity
 ahx_status wait_event(ahx_handle* h, cudaEvent_t ev, int timeout_ms);        // bounded, lock not held
 

@@ -104,5 +104,20 @@ AHX_HD inline bool block_column(const StepSplit& P, int nx, int jbase, int jhi, 
   return strip_column(P, nx, ((by - main_by) * P.gx + bx) * 32 * rows + ty * 32 + tx, i, j);
 }
 
+// The TMA-staged paired step (ws > 0 only) tiles the main columns from row m0 instead of jbase, so a block's rows are
+// rows of main columns only (its staged boxes then never start on a strip row): main blocks over rows [m0, m1), then
+// the same strip blocks as block_column.
+AHX_HD inline int staged_main_blocks_y(const StepSplit& P, int rows) { return (P.m1 - P.m0 + rows - 1) / rows; }
+AHX_HD inline bool staged_block_column(const StepSplit& P, int nx, int rows, int bx, int by, int tx, int ty, int& i,
+                                       int& j) {
+  const int main_by = staged_main_blocks_y(P, rows);
+  if (by < main_by) {
+    i = P.we + bx * 32 + tx;
+    j = P.m0 + by * rows + ty;
+    return i < P.ea && j < P.m1;
+  }
+  return strip_column(P, nx, ((by - main_by) * P.gx + bx) * 32 * rows + ty * 32 + tx, i, j);
+}
+
 
 }  // namespace ahx

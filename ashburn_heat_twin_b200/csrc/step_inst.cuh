@@ -9,6 +9,7 @@
 #include "fused.cuh"
 #include "launch.h"
 #include "tma.cuh"
+#include "tma_pairs.cuh"
 
 namespace ahx {
 namespace AHX_STEP_NS {
@@ -40,6 +41,25 @@ template <class S, int TY, int DEPTH>
 __global__ void __launch_bounds__(32 * TY, TY == 4 ? 4 : 2)
     step_tma_kernel(DomainView D, const __grid_constant__ TmaMaps M, int zslab) {
   step_tma_block<S, AHX_STEP_FAST != 0, TY, DEPTH>(D, M, zslab);
+}
+
+// Staged paired step of the 16-bit storages (FMA build): main blocks of 32 x TY columns read their interior pairs'
+// sources from TMA-staged level-pair words (tma_pairs.cuh); the strip blocks after them run the plain paired path.
+// Resident blocks per SM follow the shared memory a block takes (DEPTH stages of 14.5 KB at TY = 4, 29 KB at TY = 8)
+// and set the register budget (5 / 4 / 3 blocks of 128 threads: 96 / 128 / 168 registers).
+template <int TY, int DEPTH>
+inline constexpr int kPairStageBlocks = TY == 8 ? 2 : (DEPTH <= 2 ? 5 : (DEPTH == 3 ? 4 : 3));
+template <class S, int TY, int DEPTH>
+__global__ void __launch_bounds__(32 * TY, kPairStageBlocks<TY, DEPTH>)
+    step_pair_tma_kernel(DomainView D, const __grid_constant__ TmaMaps M, int zslab) {
+  const StepSplit SP = step_split(D.nx, D.jlo, D.jhi, D.jbase, D.jg0, D.nyg, D.strip);
+  const int mby = staged_main_blocks_y(SP, TY);
+  if ((int)blockIdx.y < mby)
+    step_pair_tma_block<S, TY, DEPTH>(D, M, SP, zslab);
+  else
+    step_block<S, 0, false, true, true>(D, blockIdx.x, (int)blockIdx.y - mby + main_blocks_y(D.jhi, D.jbase, TY),
+                                        blockIdx.z, zslab);
+  if constexpr (kDitherOf<S>) tick_done(D, gridDim.x * gridDim.y * gridDim.z);
 }
 
 // Batched step: one persistent launch steps every member domain of a batch. Blocks take tiles (32 x 4 columns x that
@@ -153,6 +173,43 @@ static cudaError_t launch_tma(const DomainView& D, const StepLaunch& L, cudaStre
   }
 }
 
+template <class S, int TY, int DEPTH>
+static cudaError_t launch_pair_tma_t(const DomainView& D, const StepLaunch& L, cudaStream_t s) {
+  if constexpr (AHX_STEP_FAST != 0) {
+    int zs = L.zslab > 0 ? L.zslab : D.nz;
+    zs = (zs + 1) & ~1;   // blocks start on an even level: a level pair is one word
+    const size_t smem = pair_stage_smem_bytes<TY, DEPTH>(D.nz);
+    static int configured[64] = {0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64 || configured[dev] < (int)smem) {
+      const cudaError_t e = cudaFuncSetAttribute(step_pair_tma_kernel<S, TY, DEPTH>,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e != cudaSuccess) return e;
+      if (dev >= 0 && dev < 64) configured[dev] = (int)smem;
+    }
+    if (D.strip <= 0) return cudaErrorInvalidValue;   // the staged tiles need the face columns in strip blocks
+    const StepSplit SP = step_split(D.nx, D.jlo, D.jhi, D.jbase, D.jg0, D.nyg, D.strip);
+    dim3 grid(SP.gx, staged_main_blocks_y(SP, TY) + strip_blocks_y(SP, TY), (D.nz + zs - 1) / zs);
+    step_pair_tma_kernel<S, TY, DEPTH><<<grid, dim3(32, TY), smem, s>>>(D, *L.maps, zs);
+    return cudaGetLastError();
+  } else {
+    return cudaErrorInvalidValue;
+  }
+}
+
+template <class S>
+static cudaError_t launch_pair_tma(const DomainView& D, const StepLaunch& L, cudaStream_t s) {
+  switch (L.tma_ty * 10 + L.tma_depth) {
+    case 42: return launch_pair_tma_t<S, 4, 2>(D, L, s);
+    case 43: return launch_pair_tma_t<S, 4, 3>(D, L, s);
+    case 44: return launch_pair_tma_t<S, 4, 4>(D, L, s);
+    case 82: return launch_pair_tma_t<S, 8, 2>(D, L, s);
+    case 83: return launch_pair_tma_t<S, 8, 3>(D, L, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
 template <class S, int MODE, bool BUDGET>
 static cudaError_t launch_t(const DomainView& D, const StepLaunch& L, cudaStream_t s) {
   if constexpr (MODE == 0 && !BUDGET && std::is_same_v<StoreF<S>, StoreG<S>> && !kDitherOf<S> &&
@@ -160,6 +217,10 @@ static cudaError_t launch_t(const DomainView& D, const StepLaunch& L, cudaStream
     // the staged kernel stages f and g with one element size, one level per box: uniform round-to-nearest storages
     // of 4- and 8-byte elements only
     if (L.tma_ty > 0 && L.maps != nullptr) return launch_tma<S>(D, L, s);
+  }
+  if constexpr (MODE == 0 && !BUDGET && AHX_STEP_FAST != 0 && kLevelPairs<StoreF<S>> && kLevelPairs<StoreG<S>>) {
+    // the staged paired step: level-paired f and g (FP16, BF16, FP16 with stochastic rounding)
+    if (L.tma_ty > 0 && L.pairs && L.maps != nullptr) return launch_pair_tma<S>(D, L, s);
   }
   const int minb = (MODE == 0 && !BUDGET) ? L.minb : 0;
   const int by = minb ? 4 : (L.block_y > 0 ? L.block_y : 4);

@@ -205,7 +205,10 @@ ahx_status ahx_accum_read(ahx_handle* h, double* surf3, double* faces, int64_t* 
  * 2000 for paired levels (two interior levels per thread on packed f32x2 arithmetic; FMA build, f32 arithmetic; the
  * results are bit-identical to unpaired), plus 10000 for an L2 prefetch of the next level's source rows (FMA build;
  * a hint that changes no result); or, for the TMA-staged kernel, 1000 + 100 x stages + rows (rows 4 with 2-4 stages,
- * rows 8 with 2-3 stages); zslab = z-slab depth in levels; 0 = keep */
+ * rows 8 with 2-3 stages; 4- and 8-byte storages); or, for the TMA-staged paired step of the 16-bit storages (FP16,
+ * BF16, FP16 with stochastic rounding; FMA build; whole domains), 2000 + 1000 + 100 x stages + rows (rows 4 or 8 with
+ * 2-4 / 2-3 stages; bit-identical to the plain paired step); zslab = z-slab depth in levels (rounded up to even for
+ * the staged paired step); 0 = keep */
 ahx_status ahx_set_launch(ahx_handle* h, int block_y, int zslab);
 /* time candidate launch shapes on scratch copies of the state and keep the fastest; the state is not advanced;
  * *best_block_y uses the encoding of ahx_set_launch */

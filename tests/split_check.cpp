@@ -1,6 +1,7 @@
 // Coverage check of the column split of a step launch (split.h), run by tests/test_split_host.py: for each
-// configuration on the command line (nx ny jg0 nyg jlo jhi jbase ws rows) it walks every thread of the launch grid the
-// step launcher builds and checks that each column of the step's rows is taken by exactly one thread, that no main
+// configuration on the command line (nx ny jg0 nyg jlo jhi jbase ws rows staged) it walks every thread of the launch
+// grid the step launcher builds (staged = 1: the TMA-staged paired step's grid, main blocks from row m0) and checks
+// that each column of the step's rows is taken by exactly one thread, that no main
 // warp holds a lateral-face column when ws > 0, and that the lanes of a main warp are 32 consecutive columns of one
 // row. Prints "ok <columns>" or the first failure.
 #include <cstdio>
@@ -11,9 +12,10 @@
 
 using namespace ahx;
 
-static int check(int nx, int ny, int jg0, int nyg, int jlo, int jhi, int jbase, int ws, int rows) {
+static int check(int nx, int ny, int jg0, int nyg, int jlo, int jhi, int jbase, int ws, int rows, int staged) {
   const StepSplit P = step_split(nx, jlo, jhi, jbase, jg0, nyg, ws);
-  const int gy = main_blocks_y(jhi, jbase, rows) + strip_blocks_y(P, rows);
+  const int main_by = staged ? staged_main_blocks_y(P, rows) : main_blocks_y(jhi, jbase, rows);
+  const int gy = main_by + strip_blocks_y(P, rows);
   std::vector<int> seen((size_t)nx * ny, 0);
   for (int by = 0; by < gy; ++by)
     for (int bx = 0; bx < P.gx; ++bx)
@@ -21,13 +23,15 @@ static int check(int nx, int ny, int jg0, int nyg, int jlo, int jhi, int jbase, 
         int row = -1, first = -1;
         for (int tx = 0; tx < 32; ++tx) {
           int i, j;
-          if (!block_column(P, nx, jbase, jhi, rows, bx, by, tx, ty, i, j)) continue;
+          const bool got = staged ? staged_block_column(P, nx, rows, bx, by, tx, ty, i, j)
+                                  : block_column(P, nx, jbase, jhi, rows, bx, by, tx, ty, i, j);
+          if (!got) continue;
           if (i < 0 || i >= nx || j < 0 || j >= ny) {
             printf("column (%d, %d) outside the domain\n", i, j);
             return 1;
           }
           ++seen[(size_t)j * nx + i];
-          const bool main = by < main_blocks_y(jhi, jbase, rows);
+          const bool main = by < main_by;
           if (main && ws > 0) {
             const int jg = j + jg0;
             if (i == 0 || i == nx - 1 || jg == 0 || jg == nyg - 1) {
@@ -59,17 +63,17 @@ static int check(int nx, int ny, int jg0, int nyg, int jlo, int jhi, int jbase, 
 }
 
 int main(int argc, char** argv) {
-  if ((argc - 1) % 9 != 0) {
-    printf("usage: split_check (nx ny jg0 nyg jlo jhi jbase ws rows)...\n");
+  if ((argc - 1) % 10 != 0) {
+    printf("usage: split_check (nx ny jg0 nyg jlo jhi jbase ws rows staged)...\n");
     return 2;
   }
   int n = 0;
-  for (int a = 1; a < argc; a += 9) {
-    int v[9];
-    for (int t = 0; t < 9; ++t) v[t] = atoi(argv[a + t]);
-    if (check(v[0], v[1], v[2], v[3], v[4], v[5], v[6], v[7], v[8])) {
-      printf("failed: nx %d ny %d jg0 %d nyg %d jlo %d jhi %d jbase %d ws %d rows %d\n", v[0], v[1], v[2], v[3], v[4],
-             v[5], v[6], v[7], v[8]);
+  for (int a = 1; a < argc; a += 10) {
+    int v[10];
+    for (int t = 0; t < 10; ++t) v[t] = atoi(argv[a + t]);
+    if (check(v[0], v[1], v[2], v[3], v[4], v[5], v[6], v[7], v[8], v[9])) {
+      printf("failed: nx %d ny %d jg0 %d nyg %d jlo %d jhi %d jbase %d ws %d rows %d staged %d\n", v[0], v[1], v[2],
+             v[3], v[4], v[5], v[6], v[7], v[8], v[9]);
       return 1;
     }
     ++n;
