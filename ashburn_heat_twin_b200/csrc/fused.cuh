@@ -688,33 +688,118 @@ __device__ __forceinline__ void fast_pair_relax(const DomainView& D, const Param
       });
 }
 
+// The 38 pull-source words of an interior level pair (k, k + 1), k even, of a storage whose f and g planes are both
+// level-paired (FP16, BF16, FP16 with stochastic rounding), t = k / 2: for population slot p (f: q, g: 19 + q) slot
+// pair_slot(p) holds the first source word (word t of the source column for cz = 0 and cz = -1, word t - 1 for
+// cz = +1) and, when the population moves vertically, the next slot its second word (one pair up: word t for cz = +1,
+// word t + 1 for cz = -1). The pair may be the lid pair (k + 1 the
+// top level, nz even): the cz = -1 sources of the top cell are then, for f, the free-slip mirror, the cz = +1
+// partner's population at the same lateral source and level (kernel.js:168-181), i.e. the high half of the partner's
+// second word, which the second slot then holds; for g the own value (zero gradient), the high half of the first word,
+// which the second slot then repeats. Every load is issued unconditionally, so all 38 are in flight together.
+constexpr int kPairSlots = 38;
+__host__ __device__ constexpr int pair_slot(int p) {
+  int s = 0;
+  for (int a = 0; a < p; ++a) s += 1 + ((a < 19 ? kC19[a][2] : kC7[a - 19][2]) != 0 ? 1 : 0);
+  return s;
+}
+static_assert(pair_slot(26) == kPairSlots, "38 words per level pair");
+
+template <class S>
+__device__ __forceinline__ void pair_words_load(const DomainView& D, int k, uint32_t mc, uint32_t (&w)[kPairSlots]) {
+  using TF = StoreF<S>;
+  using TG = StoreG<S>;
+  const uint32_t ps = D.ps;
+  const uint32_t nf = lvl<TF>(k, mc, ps), ng = lvl<TG>(k, mc, ps);
+  const bool top = k + 1 == D.nz - 1;
+  static_for<19>([&](auto Q) {
+    constexpr int q = Q;
+    constexpr int cz = kC19[q][2];
+    constexpr int sl = pair_slot(q);
+    const TF* src = static_cast<const TF*>(D.src_f[q]) + nf;
+    w[sl] = CodecF<S>::load_w(src);
+    if constexpr (cz == 1) w[sl + 1] = CodecF<S>::load_w(src + 2u * ps);
+    if constexpr (cz == -1) {
+      // at the lid: the mirror's second word (its pull source has the same lateral shift)
+      const TF* base2 = static_cast<const TF*>(top ? D.src_f[mirz19(q)] : D.src_f[q]);
+      w[sl + 1] = CodecF<S>::load_w(base2 + nf + 2u * ps);
+    }
+  });
+  static_for<7>([&](auto Q) {
+    constexpr int q = Q;
+    constexpr int cz = kC7[q][2];
+    constexpr int sl = pair_slot(19 + q);
+    const TG* src = static_cast<const TG*>(D.src_g[q]) + ng;
+    w[sl] = CodecG<S>::load_w(src);
+    if constexpr (cz == 1) w[sl + 1] = CodecG<S>::load_w(src + 2u * ps);
+    if constexpr (cz == -1) w[sl + 1] = CodecG<S>::load_w(src + (top ? 0u : 2u * ps));
+  });
+}
+
+// relax the pair (k, k + 1) from its 38 words (pair_words_load): both cells' sources joined per population by one byte
+// permutation, decoded and relaxed as fast_pair_relax does
+template <class S>
+__device__ __forceinline__ void pair_words_relax(const DomainView& D, const ParamsHead& P, const RelaxConst& RK,
+                                                 const float4* prof, const Column<float>& C, int k, uint32_t mc,
+                                                 const uint32_t (&w)[kPairSlots], uint32_t r0, uint32_t r1) {
+  using TF = StoreF<S>;
+  using TG = StoreG<S>;
+  const uint32_t ps = D.ps;
+  const uint32_t nf = lvl<TF>(k, mc, ps), ng = lvl<TG>(k, mc, ps);
+  const bool top = k + 1 == D.nz - 1;
+  // cz = -1: (high of the first word, low of the second), at the lid (high, high of the second); cz = +1 always
+  // (high of the first, low of the second)
+  const uint32_t sel = top ? 0x7632u : 0x5432u;
+  float2 f[19], g[7];
+  static_for<26>([&](auto Pi) {
+    constexpr int p = Pi;
+    constexpr bool isf = p < 19;
+    constexpr int q = isf ? p : p - 19;
+    constexpr int cz = isf ? kC19[q][2] : kC7[q][2];
+    constexpr int sl = pair_slot(p);
+    uint32_t x = w[sl];
+    if constexpr (cz == 1) x = __byte_perm(w[sl], w[sl + 1], 0x5432);
+    if constexpr (cz == -1) x = __byte_perm(w[sl], w[sl + 1], sel);
+    if constexpr (isf) f[q] = word_dec_f<TF>(x, (float)w19(q));
+    else g[q] = word_dec_g<TG>(x);
+  });
+  fast_pair_relax<S>(D, P, RK, prof, C, k, nf, ng, f, g, r0, r1);
+}
+
 // Two vertically adjacent interior cells (k, k + 1) of one column, streamed and relaxed as the two lanes of packed
 // f32x2 arithmetic (mc = j px + i; k even when a population plane is level-paired: then each population of the two
-// cells is one word). Interior cells are never the first fluid cell (no drag, no source); the result of each lane is bit-identical
-// to stream_interior + fast_update on that cell alone.
+// cells is one word, and with level-paired f and g the pair may be the lid pair, pair_words_load). Interior cells are
+// never the first fluid cell (no drag, no source); the result of each lane is bit-identical to stream_interior or
+// stream_cell + fast_update on that cell alone.
 template <class S>
 __device__ __forceinline__ void fast_pair(const DomainView& D, const ParamsHead& P, const RelaxConst& RK,
                                           const float4* prof, const Column<float>& C, int k, uint32_t mc, uint32_t r0,
                                           uint32_t r1) {
   using TF = StoreF<S>;
   using TG = StoreG<S>;
-  const uint32_t ps = D.ps;
-  // own element offsets: the pair's word in a level-paired plane (lvl of the even level k), else level k's cell
-  const uint32_t nf = lvl<TF>(k, mc, ps), ng = lvl<TG>(k, mc, ps);
-  float2 f[19], g[7];
-  static_for<19>([&](auto Q) {
-    constexpr int q = Q;
-    const TF* src = static_cast<const TF*>(D.src_f[q]) + nf;
-    if constexpr (kLevelPairs<TF>) f[q] = word_load_f<kC19[q][2] != 0>(src, ps, (float)w19(q));
-    else f[q] = pair_load_f(src, ps, (float)w19(q));
-  });
-  static_for<7>([&](auto Q) {
-    constexpr int q = Q;
-    const TG* src = static_cast<const TG*>(D.src_g[q]) + ng;
-    if constexpr (kLevelPairs<TG>) g[q] = word_load_g<kC7[q][2] != 0>(src, ps);
-    else g[q] = pair_load_g(src, ps);
-  });
-  fast_pair_relax<S>(D, P, RK, prof, C, k, nf, ng, f, g, r0, r1);
+  if constexpr (kLevelPairs<TF> && kLevelPairs<TG>) {
+    uint32_t w[kPairSlots];
+    pair_words_load<S>(D, k, mc, w);
+    pair_words_relax<S>(D, P, RK, prof, C, k, mc, w, r0, r1);
+  } else {
+    const uint32_t ps = D.ps;
+    // own element offsets: the pair's word in a level-paired f plane (lvl of the even level k), else level k's cell
+    const uint32_t nf = lvl<TF>(k, mc, ps), ng = lvl<TG>(k, mc, ps);
+    float2 f[19], g[7];
+    static_for<19>([&](auto Q) {
+      constexpr int q = Q;
+      const TF* src = static_cast<const TF*>(D.src_f[q]) + nf;
+      if constexpr (kLevelPairs<TF>) f[q] = word_load_f<kC19[q][2] != 0>(src, ps, (float)w19(q));
+      else f[q] = pair_load_f(src, ps, (float)w19(q));
+    });
+    static_for<7>([&](auto Q) {
+      constexpr int q = Q;
+      const TG* src = static_cast<const TG*>(D.src_g[q]) + ng;
+      if constexpr (kLevelPairs<TG>) g[q] = word_load_g<kC7[q][2] != 0>(src, ps);
+      else g[q] = pair_load_g(src, ps);
+    });
+    fast_pair_relax<S>(D, P, RK, prof, C, k, nf, ng, f, g, r0, r1);
+  }
 }
 
 // Population slot p of a cell update: f population p (p < 19) or g population p - 19 (p < 26). Bit p of these masks
@@ -826,6 +911,7 @@ __device__ __forceinline__ void step_block(const DomainView& D, int bx, int by, 
   constexpr bool kPairs = PAIRS && FAST && MODE == 0 && !BUDGET && std::is_same_v<R, float>;
   // a level-paired plane pairs the levels (2t, 2t + 1) only: an odd first level runs alone
   constexpr bool kEvenPairs = kLevelPairs<StoreF<S>> || kLevelPairs<StoreG<S>>;
+  constexpr bool kLidPairs = kLevelPairs<StoreF<S>> && kLevelPairs<StoreG<S>>;
   // FMA build, plain steps, launch option: the next level's (pair's) source rows are prefetched into L2 one level
   // (pair) ahead
   constexpr bool kPrefetch = FAST && MODE == 0 && !BUDGET;   // (main blocks only: strip lanes are not one row)
@@ -840,7 +926,8 @@ __device__ __forceinline__ void step_block(const DomainView& D, int bx, int by, 
     }
     if constexpr (kPairs) {
       if (k + 1 < k1 && (!kEvenPairs || (k & 1) == 0)) {
-        const bool in2 = valid && k >= C.kg && !C.face && k >= C.kint && k + 1 < D.nz - 1;
+        // level-paired f and g also pair the lid level with the one below it (fast_pair)
+        const bool in2 = valid && k >= C.kg && !C.face && k >= C.kint && k + 1 < D.nz - (kLidPairs ? 0 : 1);
         const unsigned m2 = __ballot_sync(0xffffffffu, valid && k + 1 >= C.kg);
         if (m2 != 0u && __ballot_sync(0xffffffffu, in2) == m2) {
           if (in2) fast_pair<S>(D, P, RK, smem_prof, C, k, base, seed(k), seed(k + 1));

@@ -31,11 +31,13 @@ __device__ __forceinline__ double vsqrt(double a) { return sqrt(a); }
 __device__ __forceinline__ float2 vfma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
 __device__ __forceinline__ float2 vmul(float2 a, float2 b) { return __fmul2_rn(a, b); }
 __device__ __forceinline__ float2 vadd(float2 a, float2 b) { return __fadd2_rn(a, b); }
-__device__ __forceinline__ float2 vsub(float2 a, float2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
+// a - b as one packed multiply-add, b (-1) + a: the product is exact, so each lane rounds exactly like a - b (a
+// negated operand would cost two scalar negations first)
+__device__ __forceinline__ float2 vsub(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.0f, -1.0f), a); }
 __device__ __forceinline__ float2 vrcp(float2 a) { return make_float2(vrcp(a.x), vrcp(a.y)); }
 __device__ __forceinline__ float vneg(float a) { return -a; }
 __device__ __forceinline__ double vneg(double a) { return -a; }
-__device__ __forceinline__ float2 vneg(float2 a) { return make_float2(-a.x, -a.y); }
+__device__ __forceinline__ float2 vneg(float2 a) { return __fmul2_rn(a, make_float2(-1.0f, -1.0f)); }
 __device__ __forceinline__ float2 vsqrt(float2 a) { return make_float2(vsqrt(a.x), vsqrt(a.y)); }
 
 // a constant in lane type V

@@ -221,8 +221,9 @@ def test_launch_shapes_bit_exact(shape, zslab):
 @pytest.mark.parametrize('precision', ['fp32', 'fp16', 'fp16g32', 'fp16sr'])
 def test_paired_levels_bit_identical(precision):
     """The FMA build's paired path (two interior levels per thread on packed f32x2 arithmetic, launch shapes
-    2404 / 2504 / 2604) and the L2-prefetch option (10000 +) leave exactly the state and outputs of the unpaired
-    path, with whole columns and with odd z-slabs (which change how levels pair)."""
+    2404 / 2504 / 2604; with 16-bit f and g the lid level pairs with the one below it, nz = 30 here) and the
+    L2-prefetch option (10000 +) leave exactly the state and outputs of the unpaired path, with whole columns and
+    with odd z-slabs (which change how levels pair)."""
     met = dict(u10=5.0, dirFrom=300.0, wstar=1.5, blh=700.0)
     ref = small_solver(cuda_backend(precision, 'fast'), met=met)
     ref._dev.set_launch(404, 0)
