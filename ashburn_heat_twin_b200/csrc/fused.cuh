@@ -334,12 +334,13 @@ __device__ __forceinline__ void stream_interior(const DomainView& D, const float
   X.vI = R(pr.y);
   X.kb = R(pr.z);
   const uint32_t ps = D.ps, px = (uint32_t)D.px, n = (uint32_t)k * ps + m;
+  const uint32_t nf = lvl<TF>(k, m, ps), ng = lvl<TG>(k, m, ps);
   static_for<19>([&](auto Q) {
     constexpr int q = Q;
     [[maybe_unused]] constexpr int cx = kC19[q][0], cy = kC19[q][1], cz = kC19[q][2];
     if constexpr (kLevelPairs<TF>)
       X.f[q] = KF::dec_f(KF::load(static_cast<const TF*>(D.fA) +
-                                  ((uint32_t)q * D.qs + lvl_nbr<TF>(k, m, 0u, cz, (uint32_t)(cx + cy * (int)px), ps))),
+                                  ((uint32_t)q * D.qs + lvl_nbr<TF>(k, m, nf, cz, (uint32_t)(cx + cy * (int)px), ps))),
                          R(w19(q)));
     else
       X.f[q] = KF::dec_f(KF::load(static_cast<const TF*>(D.src_f[q]) + n), R(w19(q)));
@@ -349,7 +350,7 @@ __device__ __forceinline__ void stream_interior(const DomainView& D, const float
     [[maybe_unused]] constexpr int cx = kC7[q][0], cy = kC7[q][1], cz = kC7[q][2];
     if constexpr (kLevelPairs<TG>)
       X.g[q] = KG::dec_g(KG::load(static_cast<const TG*>(D.gA) +
-                                  ((uint32_t)q * D.qs + lvl_nbr<TG>(k, m, 0u, cz, (uint32_t)(cx + cy * (int)px), ps))));
+                                  ((uint32_t)q * D.qs + lvl_nbr<TG>(k, m, ng, cz, (uint32_t)(cx + cy * (int)px), ps))));
     else
       X.g[q] = KG::dec_g(KG::load(static_cast<const TG*>(D.src_g[q]) + n));
   });

@@ -287,8 +287,18 @@ __host__ __device__ __forceinline__ uint32_t lvl(int k, uint32_t m, uint32_t ps)
 // element offset of the neighbour (k - cz, m - d) of the cell (k, m) whose own offset is n (= lvl<T>(k, m, ps))
 template <class T>
 __host__ __device__ __forceinline__ uint32_t lvl_nbr(int k, uint32_t m, uint32_t n, int cz, uint32_t d, uint32_t ps) {
-  if constexpr (kLevelPairs<T>) return lvl<T>(k - cz, m - d, ps);
-  else return n - (d + (uint32_t)(cz * (int)ps));
+  if constexpr (kLevelPairs<T>) {
+    // from the own offset n: the lateral shift moves 2 d elements; level k - cz is the other half of the own word
+    // (k even, cz = -1: + 1; k odd, cz = +1: - 1) or a half of the word one pair down / up (k even, cz = +1:
+    // + 1 - 2 ps; k odd, cz = -1: - 1 + 2 ps). Equal to lvl(k - cz, m - d) (m is implied by n)
+    (void)m;
+    const uint32_t dz = cz == 0 ? 0u
+                        : cz > 0 ? ((k & 1) ? 0xFFFFFFFFu : 1u - 2u * ps)
+                                 : ((k & 1) ? 2u * ps - 1u : 1u);
+    return n - 2u * d + dz;
+  } else {
+    return n - (d + (uint32_t)(cz * (int)ps));
+  }
 }
 
 // Storage of a state: a plain type stores f and g alike; Mixed<SF, SG> stores the flow populations f as SF and the
