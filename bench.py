@@ -252,10 +252,11 @@ def secondary_rates(a, local):
         s._dev.time_steps(a.warmup)
         ms = s._dev.time_steps(a.steps) / a.steps
         cells, fluid = s.info['nCells'], s.info['nFluid']
+        traffic, traffic_src = profile_traffic(p, (by, zs), fluid)
         out[p] = dict(glups=cells / ms / 1e6, ms_per_step=ms, launch=dict(block_y=by, zslab=zs),
                       roofline=dict(bound='hbm', achieved=fluid * CELL_BYTES[p] / (ms / 1e3) / 1e9, peak=peak,
                                     unit='GB/s', frac=fluid * CELL_BYTES[p] / (ms / 1e3) / 1e9 / peak,
-                                    peak_source=peak_kind),
+                                    traffic=traffic, traffic_source=traffic_src, peak_source=peak_kind),
                       dtype=DTYPE[p])
         s.destroy()
     st = synth.make_static10(synth.C1)
