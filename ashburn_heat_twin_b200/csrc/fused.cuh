@@ -945,14 +945,21 @@ __device__ __forceinline__ void step_block(const DomainView& D, int bx, int by, 
       const uint32_t n = (uint32_t)k * D.ps + base;   // the cell in [k][j][px] order (output modes)
       const uint32_t nf = lvl<StoreF<S>>(k, base, D.ps), ng = lvl<StoreG<S>>(k, base, D.ps);
       Cell<R> X;
-      if (all_inter) stream_interior<S>(D, smem_prof, C, k, base, X);
-      else stream_cell<S>(D, P, smem_prof, C, k, base, X);
+      // paired kernels of the 16-bit storages: the single-level cells (a small share) read their column record again
+      // (cached), so the column data only they use (the 3x3 neighbour heights, the face flags, drag and source) is
+      // not held in registers across the level loop: the paired path then fits 80 registers (6 blocks per SM)
+      constexpr bool kReload = kPairs && kLidPairs;
+      Column<R> Cr;
+      if constexpr (kReload) load_column(D, P, i, j, Cr);
+      const Column<R>& Cs = kReload ? Cr : C;
+      if (all_inter) stream_interior<S>(D, smem_prof, Cs, k, base, X);
+      else stream_cell<S>(D, P, smem_prof, Cs, k, base, X);
       Macro<R> M;
       if constexpr (FAST) {
-        fast_update<S>(D, P, RK, C, k, nf, ng, X, M, seed(k));
+        fast_update<S>(D, P, RK, Cs, k, nf, ng, X, M, seed(k));
       } else {
-        moments_forces<R>(P, C, k, D.nz, X, M);
-        collide_store<S>(D, P, C, k, nf, ng, X, M, seed(k));
+        moments_forces<R>(P, Cs, k, D.nz, X, M);
+        collide_store<S>(D, P, Cs, k, nf, ng, X, M, seed(k));
       }
       if constexpr (MODE == 1) {
         D.dbg[n] = make_float4((float)M.th, (float)M.ux, (float)M.uy, (float)M.uz);
