@@ -88,10 +88,32 @@ struct Column {
   int kint;              // first level whose whole 3x3x3 neighbourhood is fluid (interior fast path from here)
 };
 
+// The column records and the ktop plane are read by every z-slab block of a column (and again by the single-level
+// cells of the 16-bit paired kernels), a few MB against the GBs of populations streaming through L2 each step: their
+// loads carry an L2 evict-last policy so they stay resident (a cache hint; no value changes).
+__device__ __forceinline__ uint64_t l2_keep_policy() {
+  uint64_t pol;
+  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+  return pol;
+}
+__device__ __forceinline__ uint4 ldg_keep(const uint4* p, uint64_t pol) {
+  uint4 v;
+  asm("ld.global.nc.L2::cache_hint.v4.u32 {%0, %1, %2, %3}, [%4], %5;"
+      : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+      : "l"(p), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ uint32_t ldg_keep(const uint32_t* p, uint64_t pol) {
+  uint32_t v;
+  asm("ld.global.nc.L2::cache_hint.u32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(pol));
+  return v;
+}
+
 template <class R>
 __device__ __forceinline__ void load_column(const DomainView& D, const ParamsHead& P, int i, int j, Column<R>& C) {
   const int nx = D.nx, ny = D.ny;
-  const uint4 cv = __ldg(D.colv + (size_t)j * nx + i);
+  const uint64_t pol = l2_keep_policy();
+  const uint4 cv = ldg_keep(D.colv + (size_t)j * nx + i, pol);
   C.i = i;
   C.j = j;
   C.ktc = (int)cv.x;
@@ -104,7 +126,7 @@ __device__ __forceinline__ void load_column(const DomainView& D, const ParamsHea
   for (int ox = 0; ox < 3; ++ox)
 #pragma unroll
     for (int oy = 0; oy < 3; ++oy)
-      C.kn[ox][oy] = (ox == 1 && oy == 1) ? C.kg : (int)__ldg(D.ktop + (size_t)ys[oy] * nx + xs[ox]);
+      C.kn[ox][oy] = (ox == 1 && oy == 1) ? C.kg : (int)ldg_keep(D.ktop + (size_t)ys[oy] * nx + xs[ox], pol);
   int km = C.kg;
 #pragma unroll
   for (int ox = 0; ox < 3; ++ox)
