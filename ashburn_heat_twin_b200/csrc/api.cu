@@ -1151,9 +1151,9 @@ ahx_status ahx_autotune(ahx_handle* h, int steps_per_trial, int* best_block_y, i
       shapes.push_back(sh);
   // The TMA-staged kernels are not candidates. The single-level one never won a trial (16-20 against 26.6 GLUPS on
   // 600x600x64) and an early build of it once stopped with a misaligned-address error whose cause was not found; the
-  // staged paired step of the 16-bit storages runs 27.6-29.1 against 36.1 GLUPS for the plain paired step there (half
-  // the resident warps, a block barrier per level pair). Both stay reachable only through explicit ahx_set_launch
-  // values.
+  // staged paired step of the 16-bit storages runs 0.76-0.81 of the plain paired step's rate there (27.6-29.1 against
+  // 36.1 GLUPS when measured: half the resident warps, a block barrier per level pair). Both stay reachable only
+  // through explicit ahx_set_launch values.
   // thin slabs put more blocks in flight on small grids, where one 6-level wave leaves the SMs latency-bound
   std::vector<int> zss = {h->dims.nz, 32, 16, 12, 8, 6, 4, 3, 2};
   DomainView D = view(h);
