@@ -721,7 +721,7 @@ __device__ __forceinline__ void fast_pair_relax(const DomainView& D, const Param
 // second word, which the second slot then holds; for g the own value (zero gradient), the high half of the first word,
 // which the second slot then repeats. Every load is issued unconditionally, so all 38 are in flight together.
 constexpr int kPairSlots = 38;
-__host__ __device__ constexpr int pair_slot(int p) {
+constexpr int pair_slot(int p) {   // evaluated at compile time (constant expressions only)
   int s = 0;
   for (int a = 0; a < p; ++a) s += 1 + ((a < 19 ? kC19[a][2] : kC7[a - 19][2]) != 0 ? 1 : 0);
   return s;
