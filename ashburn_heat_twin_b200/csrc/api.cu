@@ -88,7 +88,7 @@ DomainView ahx::view_at(ahx_handle* h, int parity) {
   D.jlo = slab ? h->jlo : 0;
   D.jhi = slab ? h->jhi : h->dims.ny;
   D.jbase = 0;
-  D.strip = strip_width(h->esize);
+  D.strip = strip_width(h->esize, h->dims.nx);
   D.ps = h->ps;
   D.qs = h->qs;
   set_offsets(D, h->esize, h->esize_g);

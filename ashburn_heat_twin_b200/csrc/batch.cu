@@ -284,7 +284,7 @@ struct TileGrid {
 };
 TileGrid tile_grid(const ahx_handle* h) {
   const int nx = h->dims.nx, ny = h->dims.ny;
-  const StepSplit SP = step_split(nx, 0, ny, 0, 0, ny, strip_width(h->esize));
+  const StepSplit SP = step_split(nx, 0, ny, 0, 0, ny, strip_width(h->esize, nx));
   return TileGrid{SP.gx, main_blocks_y(ny, 0, 4) + strip_blocks_y(SP, 4)};
 }
 

@@ -85,11 +85,15 @@ AHX_HD inline int strip_blocks_y(const StepSplit& P, int rows) {
   const int per = P.gx * 32 * rows, n = P.nw + P.ne + P.nsn;
   return (n + per - 1) / per;
 }
-// strip width of a storage: 16 columns when a population element is 2 bytes (32-byte sectors of 16-bit planes; the
-// main path of the 16-bit storages is bound by instruction issue, so taking its face columns off the main warps pays),
-// else none (the 4- and 8-byte storages are bound by DRAM bandwidth, and sector-aligned main warps keep every write
-// a whole sector)
-AHX_HD constexpr int strip_width(int esize_f) { return esize_f == 2 ? 16 : 0; }
+// strip width of a storage on a grid nx columns wide: for 2-byte population elements 8 or 16 columns, whichever leaves
+// fewer columns to the strips (the 16-bit planes keep two levels of a column in one 4-byte word, so 8 columns are
+// one 32-byte sector; the main path of the 16-bit storages is bound by instruction issue, so taking its face columns
+// off the main warps pays; ties keep 16), else none (the 4- and 8-byte storages are bound by DRAM bandwidth, and
+// sector-aligned main warps keep every write a whole sector)
+AHX_HD constexpr int strip_columns(int nx, int we) { return nx - 1 < we ? nx : nx - 32 * ((nx - 1 - we) / 32); }
+AHX_HD constexpr int strip_width(int esize_f, int nx) {
+  return esize_f != 2 ? 0 : (strip_columns(nx, 8) < strip_columns(nx, 16) ? 8 : 16);
+}
 
 // the column (i, j) of thread (tx, ty) of block (bx, by) of a step launch with `rows` rows per block over rows
 // [jbase, jhi): main blocks first (by < main_blocks_y), strip blocks after them; false for a thread without a column

@@ -51,8 +51,8 @@ def small_static(seed=5, ncols=64, nrows=48, buildings=60):
     return synth.make_static10(spec2) if buildings else st
 
 
-def small_solver(backend, seed=5, dx=10, heightM=300, met=None, **kw):
-    st = small_static(seed=seed)
+def small_solver(backend, seed=5, dx=10, heightM=300, met=None, ncols=64, nrows=48, **kw):
+    st = small_static(seed=seed, ncols=ncols, nrows=nrows)
     o = dict(static=st, dx=dx, allowAnyDx=True, heightM=heightM, u10Max=8,
              met=met or dict(u10=4.0, dirFrom=250.0, wstar=1.2, blh=800.0), existingFlux=400)
     o.update(kw)

@@ -143,6 +143,31 @@ def test_fp64_build_bit_exact_with_fp64_oracle():
     o.destroy()
 
 
+def test_16bit_narrow_strips_300_wide():
+    """A grid 300 columns wide takes 8-column strips with 16-bit storage (12 strip columns per row instead of 44 with
+    16): the FMA build's paired step (tuned launch) stays bit-identical to its unpaired step, and within the 16-bit bar
+    of the FP64 build after 200 steps, so every column is stepped exactly once."""
+    met = dict(u10=5.0, dirFrom=250.0, wstar=1.5, blh=700.0)
+    kw = dict(met=met, ncols=300, nrows=40)
+    p = small_solver(cuda_backend('fp16', 'fast'), **kw)
+    u = small_solver(cuda_backend('fp16', 'fast'), **kw)
+    d = small_solver(cuda_backend('fp64', 'exact'), **kw)
+    assert p.info['nx'] == 300
+    p._dev.autotune(2)
+    u._dev.set_launch(404, 0)
+    for s in (p, u, d):
+        s._dbg.stepOut(200).result()
+    fp, gp = p._dev.read_state()
+    fu, gu = u._dev.read_state()
+    assert np.array_equal(fp.view(np.uint32), fu.view(np.uint32)) and np.array_equal(gp.view(np.uint32),
+                                                                                      gu.view(np.uint32))
+    a, b = p._dbg.readDbg().reshape(-1, 4), d._dbg.readDbg().reshape(-1, 4)
+    fl = b[:, 0] != 0
+    assert rel_l2(a[fl, 0], b[fl, 0]) <= 1e-3
+    for s in (p, u, d):
+        s.destroy()
+
+
 @pytest.mark.parametrize('precision,tol', [('fp16', 1e-3), ('bf16', 2e-2), ('fp16g32', 1e-3), ('bf16g32', 2e-2),
                                            ('fp16sr', 1e-3)])
 def test_16bit_storage_error_vs_fp64(precision, tol):

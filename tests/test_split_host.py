@@ -55,11 +55,11 @@ def test_slabs_and_bands(split_check):
 
 
 def test_staged_grid(split_check):
-    """The TMA-staged paired step's grid (main blocks from the first main row, 16-column strips): whole domains and
-    y-slabs, every column exactly once, no face column in a main warp."""
-    cases = [(nx, ny, 0, ny, 0, ny, 0, 16, rows, 1)
+    """The TMA-staged paired step's grid (main blocks from the first main row, 8- or 16-column strips): whole domains
+    and y-slabs, every column exactly once, no face column in a main warp."""
+    cases = [(nx, ny, 0, ny, 0, ny, 0, ws, rows, 1)
              for nx, ny in [(17, 3), (33, 9), (48, 5), (49, 4), (64, 3), (100, 11), (200, 13), (300, 300), (600, 6)]
-             for rows in (4, 8)]
+             for rows in (4, 8) for ws in (8, 16)]
     for nyg, parts, nx in itertools.product((12, 19), (1, 2, 3), (20, 40, 70)):
         edges = [round(nyg * p / parts) for p in range(parts + 1)]
         for a, b in zip(edges[:-1], edges[1:]):
