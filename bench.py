@@ -105,21 +105,24 @@ def measured_peaks():
 
 
 def profile_traffic(precision, launch, fluid):
-    """DRAM bytes per launch of the step kernel from the committed ncu summary of the same storage, arithmetic and
-    launch shape (profiles/step_<precision>_traffic.json), scaled by fluid cells to this launch. Returns (bytes,
-    source note); bytes is None when no capture of this launch shape exists."""
+    """DRAM bytes per launch of the step kernel from the committed ncu summaries of the same storage, arithmetic and
+    launch shape (profiles/step_<precision>_traffic.json: one capture, or a list of captures of several launch
+    shapes), scaled by fluid cells to this launch. Returns (bytes, source note); bytes is None when no capture of this
+    launch shape exists."""
     p = os.path.join(ROOT, 'profiles', f'step_{precision}_traffic.json')
     try:
-        d = json.load(open(p))
+        caps = json.load(open(p))
     except Exception:
         return None, 'no ncu capture committed for this storage'
-    got = (d.get('block_y'), d.get('zslab'))
-    if launch is None or tuple(launch) != got:
-        return None, (f'the committed capture is of launch {got[0]} / zslab {got[1]}, not the timed launch '
-                      f'{launch[0] if launch else None} / zslab {launch[1] if launch else None}')
-    return d['dram_bytes_per_fluid_cell'] * fluid, (
-        f"ncu dram__bytes_read.sum + dram__bytes_write.sum of the same launch shape on {d['grid']} "
-        f"({d['dram_bytes_per_fluid_cell']:.1f} B per fluid cell), scaled by fluid cells")
+    caps = caps if isinstance(caps, list) else [caps]
+    for d in caps:
+        if launch is not None and tuple(launch) == (d.get('block_y'), d.get('zslab')):
+            return d['dram_bytes_per_fluid_cell'] * fluid, (
+                f"ncu dram__bytes_read.sum + dram__bytes_write.sum of the same launch shape on {d['grid']} "
+                f"({d['dram_bytes_per_fluid_cell']:.1f} B per fluid cell), scaled by fluid cells")
+    have = ', '.join(f"{d.get('block_y')} / zslab {d.get('zslab')}" for d in caps)
+    return None, (f'the committed captures are of launch {have}, not the timed launch '
+                  f'{launch[0] if launch else None} / zslab {launch[1] if launch else None}')
 
 
 class Clocks:
