@@ -106,7 +106,7 @@ def test_write_state_roundtrip_and_step():
 
 
 def test_fast_arithmetic_within_tolerance():
-    """The FMA-contracted build: single-step theta rel-L2 <= 1e-5 against the oracle (the north-star parity bar),
+    """The FMA-contracted build: single-step theta rel-L2 <= 1e-5 against the oracle (the single-step parity bar),
     and <= 1e-4 after 200 steps."""
     met = dict(u10=5.0, dirFrom=250.0, wstar=1.5, blh=700.0)
     f = small_solver(cuda_backend('fp32', 'fast'), met=met)
